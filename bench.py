@@ -1,0 +1,403 @@
+#!/usr/bin/env python3
+"""Throughput of the SU(2) pure-gauge hot path on B200 -- one JSON line on rank 0.
+
+Workload (the headline metric's configuration): a 48^4 SU(2) lattice at beta = 3.09, Haar-random
+(hot) start from Philox, links in FP32.  One step = one sweep of 1 checkerboard heatbath + 4
+overrelaxation passes over all 4V links, followed by the plaquette (the reference's
+qcd.c:54-60 loop: gaugefieldUpdate then plaquette).  `value` is heatbath+overrelaxation link
+updates per second over all GPUs (5 * 4V updates per step per GPU).  The same run also reports
+APE_all / spatial-APE steps per second, the FP64 figures, W(R<=9,T<=9) sweeps and Q per second.
+
+Multi-GPU: independent replicas (one lattice per GPU, different seed), no data-path collective;
+the job aggregate is the sum of per-GPU work divided by the slowest rank's time.
+
+--impl reference times the reference's own C code (compiled from source into oracle/_ref by
+oracle/build_ref.sh) on the host cores: one independent process per core running the reference's
+localHeatbathUpdate over a bounded slice of the same 48^4 lattice each step.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "link updates/s & APE steps/s at 48^4, FP32 vs FP64 GPU, % HBM roofline"
+UNIT = "link-updates/s"
+BETA = 3.09
+N_OR = 4
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ------------------------------------------------------------------ helpers ---
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--dims", default="48,48,48,48")
+    ap.add_argument("--no-extras", action="store_true", help="headline only")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+class Dist:
+    """Rank plumbing: torch.distributed over NCCL when launched by torchrun, nothing otherwise."""
+
+    def __init__(self):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.torch = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.torch = torch
+            self.dist = dist
+
+    def barrier(self):
+        if self.torch:
+            self.dist.barrier(device_ids=[self.local])
+
+    def max(self, x):
+        if not self.torch:
+            return x
+        t = self.torch.tensor([float(x)], device="cuda", dtype=self.torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x):
+        if not self.torch:
+            return x
+        t = self.torch.tensor([float(x)], device="cuda", dtype=self.torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.torch:
+            self.dist.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.f.name):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        smax = max((float(r[2]) for r in rows if r[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def dram_traffic(key):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary (profiles/dram_traffic.json)."""
+    try:
+        with open(os.path.join(REPO, "profiles", "dram_traffic.json")) as f:
+            v = json.load(f).get(key)
+        return None if v is None else float(v["bytes_per_launch"])
+    except (OSError, ValueError, KeyError, TypeError):
+        return None
+
+
+def cpu_info():
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return model, os.cpu_count() or 1
+
+
+def mem_available_gb():
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable"):
+                return int(line.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 16.0
+
+
+# ---------------------------------------------------- reference CPU baseline ---
+
+def ref_harness(dims):
+    p = os.path.join(REPO, "oracle", "_ref", "x".join(map(str, dims)), "harness")
+    return p if os.path.exists(p) else None
+
+
+def cpu_reference_rate(dims, reps, warm, sites, procs=None):
+    """Run `procs` independent reference processes, each heatbath-updating `sites` sites x 4 dirs
+    per rep with the reference's localHeatbathUpdate; returns per-rep aggregate rates."""
+    exe = ref_harness(dims)
+    model, ncpu = cpu_info()
+    vol = math.prod(dims)
+    per_proc_gb = vol * 4 * 32 * 2.2 / 1e9 + vol * 64 / 1e9 + 0.2
+    if procs is None:
+        procs = max(1, min(ncpu, int(mem_available_gb() * 0.6 / per_proc_gb)))
+    if exe:
+        kind = "reference"
+        cmds = [[exe, "bench_hb", "1", str(1 + i), str(BETA), str(sites), str(warm + reps)] for i in range(procs)]
+    else:
+        kind = "port"
+        cmds = [[sys.executable, os.path.join(REPO, "oracle", "port_bench.py"), ",".join(map(str, dims)),
+                 str(1 + i), str(BETA), str(sites), str(warm + reps)] for i in range(procs)]
+    ps = [subprocess.Popen(c, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True) for c in cmds]
+    per_rep = [0.0] * (warm + reps)
+    for p in ps:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(f"CPU baseline process failed: {p.args}")
+        for line in out.splitlines():
+            f = line.split()
+            if len(f) >= 5 and f[0] == "RESULT" and f[1] == "hb_s":
+                r, n, t = int(f[2]), int(f[3]), float(f[4])
+                per_rep[r] += n / t
+    timed = per_rep[warm:]
+    return {
+        "rates": timed, "kind": kind, "cores": procs, "model": model, "nproc": ncpu,
+        "sample": f"{procs} independent processes x {sites} sites x 4 dirs of localHeatbathUpdate per step "
+                  f"on a hot {'x'.join(map(str, dims))} lattice (beta={BETA}), heatbath only "
+                  f"(the reference has no overrelaxation)",
+    }
+
+
+def run_reference(args, dist, dims):
+    if dist.rank != 0:
+        return
+    K, W = args.steps, args.warmup
+    sites = 200_000 if math.prod(dims) > 200_000 else math.prod(dims)
+    t0 = time.time()
+    res = cpu_reference_rate(dims, K, W, sites)
+    wall = time.time() - t0
+    val = sum(res["rates"]) / len(res["rates"])
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": K,
+        "warmup": W, "ms_per_step": 1e3 * (4 * sites) / (val / res["cores"]), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (RANLUX hot start of the reference)",
+        "config": {"workload": f"{'x'.join(map(str, dims))} SU(2) beta={BETA} hot start, heatbath link updates "
+                               f"(reference CPU code, one process per core)", "dims": dims},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
+                         "sample": res["sample"], "cpu_model": res["model"], "nproc": res["nproc"]},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm ---
+
+def time_steps(lat, K, fn):
+    lat.synchronize()
+    lat.timer_begin()
+    for _ in range(K):
+        fn()
+    return lat.timer_end()
+
+
+def run_ours(args, dist, dims):
+    from masterarbeit_b200.su2g import Lattice, PinnedArray
+
+    K, W = args.steps, args.warmup
+    vol = math.prod(dims)
+    rank = dist.rank
+    peak, peak_kind = measured_peak()
+    lat = Lattice(dims, precision="fp32", beta=BETA, seed=1000 + rank, start="haar", replica=rank, device=dist.local)
+
+    def step():
+        lat.sweep(1, 1, N_OR)
+        lat.plaquette()
+
+    for _ in range(W):
+        step()
+    lat.profile(True)
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    lat.synchronize()
+    clocks.start()
+    ms = time_steps(lat, K, step)
+    clk = clocks.stop()
+    prof = lat.profile_read()
+    lat.profile(False)
+    dist.barrier()
+    ms_max = dist.max(ms)
+    upd_per_step = (1 + N_OR) * 4 * vol
+    value = upd_per_step * K * dist.world / (ms_max / 1e3)
+    launches = sum(n for n, _ in prof.values())
+    link32 = 16
+    roof = {}
+    for name, cls, units, transfers in (("overrelax", "overrelax", vol // 2, 9), ("heatbath", "heatbath", vol // 2, 8)):
+        n, tms = prof[cls]
+        if n:
+            avg = tms / n
+            alg = units * transfers * link32
+            roof[name] = {"achieved_gbs": alg / (avg / 1e3) / 1e9, "avg_launch_ms": avg, "launches": n,
+                          "alg_bytes_per_launch": alg}
+    dom = roof.get("overrelax", {})
+    traffic = dram_traffic("overrelax_fp32_" + "x".join(map(str, dims)))
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": W,
+        "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic: Philox Haar-random hot start (no checkpoints or datasets)",
+        "config": {"workload": f"{'x'.join(map(str, dims))} SU(2) beta={BETA} hot start; step = 1 heatbath + "
+                               f"{N_OR} overrelaxation checkerboard sweeps + plaquette",
+                   "dims": list(dims), "precision": "fp32 links, fp64 reductions",
+                   "l2": f"inputs larger than L2 (field {4 * vol * link32 / 1e6:.0f} MB > 126 MB)",
+                   "parallelism": f"replicas x{dist.world}"},
+        "roofline": {"bound": "hbm", "kernel": "overrelaxation pass (32 of 40 passes per step)",
+                     "achieved": dom.get("achieved_gbs"), "peak": peak, "unit": "GB/s",
+                     "frac": (dom["achieved_gbs"] / peak) if dom else None, "traffic": traffic,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback 6650 GB/s",
+                     "alg_bytes_per_launch": dom.get("alg_bytes_per_launch"), "per_kernel": roof},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+
+    extras = {}
+    if not args.no_extras:
+        # APE steps/s (FP32) and the FP64 plain form of every figure
+        for prec in ("fp32", "fp64"):
+            L = lat if prec == "fp32" else Lattice(dims, precision="fp64", beta=BETA, seed=1000 + rank,
+                                                    start="haar", replica=rank, device=dist.local)
+            lb = 16 if prec == "fp32" else 32
+            if prec == "fp64":
+                for _ in range(W):
+                    L.sweep(1, 1, N_OR)
+                L.profile(True)
+                k64 = max(3, K // 2)
+                ms64 = time_steps(L, k64, lambda: (L.sweep(1, 1, N_OR), L.plaquette()))
+                p64 = L.profile_read()
+                L.profile(False)
+                extras["fp64_link_updates_per_s"] = upd_per_step * k64 / (ms64 / 1e3)
+                n, tms = p64["overrelax"]
+                extras["fp64_overrelax_gbs"] = (vol // 2) * 9 * lb / (tms / n / 1e3) / 1e9
+            for mode, per_site in (("all", 8), ("spatial", 6)):
+                L.ape(1, 0.5, mode)
+                L.profile(True)
+                ms_ape = time_steps(L, K, lambda: L.ape(1, 0.5, mode))
+                pa = L.profile_read()
+                L.profile(False)
+                n, tms = pa["ape"]
+                extras[f"{prec}_ape_{mode}_steps_per_s"] = K / (ms_ape / 1e3)
+                extras[f"{prec}_ape_{mode}_gbs"] = vol * per_site * lb / (tms / n / 1e3) / 1e9
+                extras[f"{prec}_ape_{mode}_frac_of_peak"] = extras[f"{prec}_ape_{mode}_gbs"] / peak
+            R = [r for r in range(1, 10) for t in range(1, 10)]
+            T = [t for r in range(1, 10) for t in range(1, 10)]
+            L.wilson([1], [1])
+            t0 = time.perf_counter()
+            L.wilson(R, T)
+            extras[f"{prec}_wilson_R9T9_sweeps_per_s"] = 1.0 / (time.perf_counter() - t0)
+            L.qtop()
+            t0 = time.perf_counter()
+            L.qtop()
+            extras[f"{prec}_qtop_per_s"] = 1.0 / (time.perf_counter() - t0)
+            if prec == "fp64":
+                L.close()
+        extras["fp32_over_fp64_link_updates"] = value / dist.world / extras["fp64_link_updates_per_s"]
+        extras["fp32_over_fp64_ape_all"] = extras["fp32_ape_all_steps_per_s"] / extras["fp64_ape_all_steps_per_s"]
+    line["extras"] = extras
+
+    # end to end through the C ABI with host buffers: upload the configuration from pinned host
+    # memory (the reference's pu block, FP64 AoS), one step, read back the plaquette
+    host = PinnedArray((vol, 4, 4))
+    lat.download(host.array)
+
+    def e2e_step():
+        lat.upload(host.array)
+        lat.sweep(1, 1, N_OR)
+        lat.plaquette()
+
+    e2e_step()
+    dist.barrier()
+    t0 = time.perf_counter()
+    ms_e2e = time_steps(lat, K, e2e_step)
+    wall_e2e = time.perf_counter() - t0
+    ms_e2e = dist.max(ms_e2e)
+    line["e2e"] = {"value": upd_per_step * K * dist.world / (ms_e2e / 1e3), "unit": UNIT,
+                   "h2d_bytes_per_step": vol * 16 * 8, "d2h_bytes_per_step": 8 + 4,
+                   "host_wall_s": wall_e2e,
+                   "what": "su2g_upload_aos_f64 (pinned host FP64 field) + su2g_sweep(1 HB + 4 OR) + su2g_plaquette"}
+    host.free()
+
+    if rank == 0 and dist.world == 1 and not args.no_cpu:
+        res = cpu_reference_rate(dims, 1, 0, 200_000)
+        line["cpu_baseline"] = {"value": res["rates"][0], "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
+                                "sample": res["sample"], "cpu_model": res["model"], "nproc": res["nproc"]}
+    lat.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    dims = [int(x) for x in args.dims.split(",")]
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist, dims)
+        else:
+            run_ours(args, dist, dims)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

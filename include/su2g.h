@@ -1,0 +1,146 @@
+/*
+ * su2g.h -- C ABI of the B200 (sm_100a) SU(2) pure-gauge lattice library (libsu2g.so).
+ *
+ * The reference (daggerfall247/Masterarbeit, LGT_Code) has no plugin or FFI layer: its
+ * update and measurement routines are plain C functions over a global field `pu`
+ * (LGT_Code/include/modules.h, LGT_Code/include/headers.h:402).  Each entry point below
+ * replaces one of those routines; the comment names the reference interface it stands in
+ * for.  The shim masterarbeit_b200/shim/ref_shim.c defines the reference's own symbols on
+ * top of these calls, so the reference's drivers (LGT_Code/main/qcd.c, main_meas/meas.c,
+ * main_qtop/qtop.c) link against it unchanged.
+ *
+ * Conventions
+ *  - Every call returns an int status: 0 = OK, negative = error (SU2G_E*).  The message of
+ *    the last failure on a handle is su2g_last_error(h); failures before a handle exists
+ *    (su2g_create) are reported by su2g_last_error(NULL).
+ *  - Host arrays are plain C arrays owned by the caller.  The gauge field itself lives in
+ *    device memory owned by the handle and stays resident between calls.
+ *  - A handle owns one CUDA stream; calls on one handle are ordered on that stream.
+ *    Calls that return values to host memory synchronise that stream.  A handle is not
+ *    thread-safe; distinct handles may be used from distinct threads.
+ *  - Lattice extents dims[4] = (L_t, L_x, L_y, L_z), each even and >= 2 (the reference's
+ *    compile-time checks, LGT_Code/include/headers.h:58-69, with L_x,y,z >= 4 there).
+ *    Site index n = ((t*L_x + x)*L_y + y)*L_z + z (LGT_Code/modules/admin/init.c:741-829).
+ *  - Host field arrays use the reference's layout exactly: the block behind pu[0][0],
+ *    double[V][4][4] = site, direction (0 = t), quaternion c0..c3
+ *    (LGT_Code/modules/admin/init.c:842-858; file body of config_IO.c:95-105).
+ */
+#ifndef SU2G_H
+#define SU2G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct su2g_lattice su2g_lattice;
+
+enum su2g_status {
+    SU2G_OK = 0,
+    SU2G_EINVAL = -1,   /* bad argument */
+    SU2G_ENOMEM = -2,   /* device or pinned host allocation failed */
+    SU2G_ECUDA = -3,    /* CUDA runtime error */
+    SU2G_EDEVICE = -4,  /* a kernel reported a failure through its status word */
+    SU2G_ENODEV = -5    /* no usable sm_100 device */
+};
+
+enum su2g_precision { SU2G_FP32 = 0, SU2G_FP64 = 1 };
+
+/* Start configurations, initGaugeField (LGT_Code/modules/admin/init.c:831-869):
+ * cold = unit links; haar = four normalised N(0,1) draws per link;
+ * ref = the reference's su2RandomMatrix formula (LGT_Code/modules/random/random_su3.c:141-155). */
+enum su2g_start { SU2G_START_COLD = 0, SU2G_START_HAAR = 1, SU2G_START_REF = 2 };
+
+/* APE variants, smearing_APE_all / _spatial / _temporal (LGT_Code/modules/obs/smearing.c:74-168). */
+enum su2g_ape_mode { SU2G_APE_ALL = 0, SU2G_APE_SPATIAL = 1, SU2G_APE_TEMPORAL = 2 };
+
+/* Update kinds for su2g_update_pass. */
+enum su2g_update_kind { SU2G_HEATBATH = 0, SU2G_OVERRELAX = 1 };
+
+typedef struct su2g_params {
+    int32_t dims[4];     /* L_t, L_x, L_y, L_z (headers.h:22-25 LENGT, LENGS1-3) */
+    int32_t precision;   /* su2g_precision */
+    int32_t start;       /* su2g_start */
+    double beta;         /* runParams.beta (headers.h:347) */
+    uint64_t seed;       /* Philox key (replaces rlxd_init(2, seed), LGT_Code/main/qcd.c:36) */
+    uint32_t replica;    /* stream id mixed into every Philox counter (0 for a single lattice) */
+    int32_t device;      /* CUDA device ordinal */
+} su2g_params;
+
+/* ---- handle lifetime: initArrayOfNeighbours + initGaugeField + releaseGaugeField
+ *      (LGT_Code/modules/admin/init.c:741-869, :922-925) */
+int su2g_create(const su2g_params *params, su2g_lattice **out);
+int su2g_destroy(su2g_lattice *h);
+const char *su2g_last_error(const su2g_lattice *h);
+
+/* Re-initialise the field (initGaugeField, init.c:831-869) with a start mode and seed. */
+int su2g_start(su2g_lattice *h, int32_t start, uint64_t seed);
+
+/* Lattice facts: dims, precision, volume, heatbath sweeps done (the Philox sweep counter). */
+int su2g_info(const su2g_lattice *h, int32_t dims[4], int32_t *precision, int64_t *volume,
+              uint32_t *hb_sweeps);
+int su2g_set_beta(su2g_lattice *h, double beta);
+/* The heatbath sweep counter keys the Philox stream; setting it makes a resume bit-exact. */
+int su2g_set_sweep_counter(su2g_lattice *h, uint32_t hb_sweeps);
+
+/* ---- host <-> device field transfer: the pu[0][0] block (readConfig / writeConfig body,
+ *      LGT_Code/modules/io/config_IO.c:537-621, :40-117).  links = double[V*16]. */
+int su2g_upload_aos_f64(su2g_lattice *h, const double *links);
+int su2g_download_aos_f64(su2g_lattice *h, double *links);
+
+/* ---- updates: gaugefieldUpdate(iup, nup, utype=1, stype=0) (LGT_Code/modules/update/update.c:102-175)
+ * n_sweeps times: n_hb checkerboard heatbath sweeps (localHeatbathUpdate, heatbath.c:124-149)
+ * followed by n_or overrelaxation sweeps (new, no reference counterpart).  Every store is
+ * reprojected (replaces project_gfield_to_sun, update.c:166).  If acc_out is not NULL it
+ * receives the mean of 1/trials over all heatbath link updates (the `acc=` log value,
+ * update.c:169-173) and the call synchronises; otherwise the call only enqueues. */
+int su2g_sweep(su2g_lattice *h, int32_t n_sweeps, int32_t n_hb, int32_t n_or, double *acc_out);
+
+/* One checkerboard pass: links of direction mu and site parity `parity`, heatbath or
+ * overrelaxation.  For a heatbath pass, `sweep` is the Philox sweep index. */
+int su2g_update_pass(su2g_lattice *h, int32_t kind, int32_t mu, int32_t parity, uint32_t sweep);
+
+/* ---- observables */
+/* plaquette() (LGT_Code/modules/obs/plaquette.c:67-100): <(1/2) Re tr U_p> over 6V plaquettes. */
+int su2g_plaquette(su2g_lattice *h, double *p);
+/* smearing_APE_* (LGT_Code/modules/obs/smearing.c:74-168), in place on the handle's field. */
+int su2g_ape(su2g_lattice *h, int32_t ns, double alpha, int32_t mode);
+/* measureWilsonLoop (LGT_Code/modules/obs/wilson.c:268-324), explicit pair list:
+ * w[i] = W(R[i], T[i]); pairs in any order; the T <= L_t - 1 check of wilson.c:290-291. */
+int su2g_wilson(su2g_lattice *h, const int32_t *R, const int32_t *T, int32_t n, double *w);
+/* topologicalCharge() (LGT_Code/modules/obs/topologicalcharge.c:164-199); sum_abs (may be NULL)
+ * receives sum_x |q(x)|, the scale against which the cancellation in Q is judged. */
+int su2g_qtop(su2g_lattice *h, double *q, double *sum_abs);
+
+/* ---- Kennedy-Pendleton sampler alone (generateSU2InHeatbath_Improved, heatbath.c:76-121;
+ * the reference's sampler test LGT_Code/main_test/test.c:115-166): counts of x0 in nbins
+ * equal bins on [-1,1] for n draws at fixed alpha. */
+int su2g_kp_histogram(su2g_lattice *h, double alpha, uint64_t seed, int64_t n, int32_t nbins,
+                      int64_t *counts);
+
+/* ---- pinned (page-locked) host memory for field arrays, so that transfers run at full link
+ * speed; the reference's pu block (init.c:842-858) can live in it. */
+int su2g_host_alloc(size_t bytes, void **ptr);
+int su2g_host_free(void *ptr);
+
+/* ---- timing and profiling on the handle's stream (CUDA events). */
+int su2g_stream(su2g_lattice *h, void **cuda_stream);
+int su2g_synchronize(su2g_lattice *h);
+int su2g_timer_begin(su2g_lattice *h);
+int su2g_timer_end(su2g_lattice *h, double *ms);
+/* When enabled, every kernel launch is bracketed by events; su2g_profile_read returns, for a
+ * kernel class, the launch count and summed device time since the last reset. */
+enum su2g_kernel_class {
+    SU2G_K_HEATBATH = 0, SU2G_K_OVERRELAX = 1, SU2G_K_PLAQUETTE = 2, SU2G_K_APE = 3,
+    SU2G_K_WILSON = 4, SU2G_K_QTOP = 5, SU2G_K_REDUCE = 6, SU2G_K_OTHER = 7, SU2G_K_COUNT = 8
+};
+int su2g_profile_enable(su2g_lattice *h, int32_t enable);
+int su2g_profile_read(su2g_lattice *h, int32_t kernel_class, int64_t *launches, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SU2G_H */

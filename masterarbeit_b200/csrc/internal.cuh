@@ -1,0 +1,147 @@
+// internal.cuh -- handle state, launch/profiling helpers and compensated FP64 reductions.
+#pragma once
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "su2g.h"
+#include "su2.cuh"
+
+namespace su2g {
+
+constexpr int kBlock = 256;            // threads per CTA for the stencil kernels
+constexpr int kMaxPartials = 8192;     // per-CTA partial sums a reduction may write
+constexpr int kOutSlots = 4096;        // device result doubles per handle
+constexpr uint32_t kMaxTrials = 1u << 20;   // Kennedy-Pendleton trials before a link gives up
+
+// Status bits a kernel may raise in the handle's status word.
+enum : unsigned { kStatusKpTrials = 1u, kStatusNonFinite = 2u };
+
+// Compensated sum: value s plus running error e (TwoSum, Knuth TAOCP vol. 2, 4.2.2).
+struct DD {
+    double s, e;
+};
+
+__device__ __forceinline__ DD dd_add(DD a, DD b)
+{
+    double s = a.s + b.s;
+    double bb = s - a.s;
+    double err = (a.s - (s - bb)) + (b.s - bb);
+    DD r;
+    r.s = s;
+    r.e = err + a.e + b.e;
+    return r;
+}
+
+__device__ __forceinline__ DD dd_add(DD a, double b)
+{
+    DD t;
+    t.s = b;
+    t.e = 0.0;
+    return dd_add(a, t);
+}
+
+__device__ __forceinline__ DD dd_shfl_xor(DD v, int lane_mask)
+{
+    DD r;
+    r.s = __shfl_xor_sync(0xffffffffu, v.s, lane_mask);
+    r.e = __shfl_xor_sync(0xffffffffu, v.e, lane_mask);
+    return r;
+}
+
+__device__ __forceinline__ DD dd_warp_sum(DD v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = dd_add(v, dd_shfl_xor(v, o));
+    return v;
+}
+
+// Block-wide compensated sum; the result is valid in thread 0.  Fixed order -> deterministic.
+template <int NT>
+__device__ __forceinline__ DD dd_block_sum(DD v)
+{
+    __shared__ DD warp_part[NT / 32];
+    v = dd_warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) warp_part[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        DD w;
+        w.s = lane < NT / 32 ? warp_part[lane].s : 0.0;
+        w.e = lane < NT / 32 ? warp_part[lane].e : 0.0;
+        v = dd_warp_sum(w);
+    }
+    __syncthreads();
+    return v;
+}
+
+// Sums `nparts` per-CTA partials for `nslots` independent slots (partials[slot*stride + part])
+// into out[slot] = scale * sum.  One CTA per slot, fixed order.
+__global__ void k_finalize(const DD* __restrict__ partials, int nparts, int stride, double scale,
+                           double* __restrict__ out);
+
+}  // namespace su2g
+
+struct su2g_lattice {
+    su2g::Geom g;
+    int prec = SU2G_FP32;
+    double beta = 0.0;
+    uint64_t seed = 0;
+    uint32_t replica = 0;
+    uint32_t hb_sweeps = 0;
+    int device = 0;
+    int num_sms = 148;
+    size_t link_bytes = 16;
+    void* field = nullptr;       // 4V links, layout of su2.cuh
+    void* field_alt = nullptr;   // second field for Jacobi smearing (allocated on first use)
+    void* dirp[4] = {nullptr, nullptr, nullptr, nullptr};   // current base of each direction
+    void* altp[4] = {nullptr, nullptr, nullptr, nullptr};   // ping-pong partner of each direction
+    su2g::DD* partials = nullptr;   // kMaxPartials x kPartialSlots compensated partial sums
+    size_t partial_slots = 0;
+    double* d_out = nullptr;     // device result slots
+    double* h_out = nullptr;     // pinned host mirror of d_out
+    unsigned* d_status = nullptr;
+    double* d_aos = nullptr;     // device staging for AoS FP64 transfers
+    size_t aos_sites = 0;        // sites the staging buffer holds
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+    bool profiling = false;
+    struct Prof {
+        cudaEvent_t a, b;
+        int cls;
+    };
+    std::vector<Prof> prof_pending;
+    std::vector<cudaEvent_t> event_pool;
+    long long prof_launches[SU2G_K_COUNT] = {0};
+    double prof_ms[SU2G_K_COUNT] = {0};
+    char err[512] = {0};
+};
+
+namespace su2g {
+
+int set_error(su2g_lattice* h, int code, const char* fmt, ...);
+int check_cuda(su2g_lattice* h, cudaError_t e, const char* what);
+
+// Number of CTAs for a grid-stride kernel over `work` items: at most `per_sm` resident CTAs
+// on every SM, never more than needed, never more than kMaxPartials.
+int grid_for(const su2g_lattice* h, long long work, int per_sm);
+
+// Bracket a launch with profiling events when profiling is on; check the launch.
+int launch_begin(su2g_lattice* h, int cls);
+int launch_end(su2g_lattice* h, int cls, const char* what);
+
+// Make sure the partial-sum scratch holds `slots` x kMaxPartials entries.
+int ensure_partials(su2g_lattice* h, size_t slots);
+// Launch k_finalize over `nslots` slots of `nparts` partials into d_out[out_off ...].
+int finalize(su2g_lattice* h, int nparts, int nslots, double scale, int out_off);
+// Copy n result doubles from d_out[off] to h_out and synchronise; then check the status word.
+int fetch_results(su2g_lattice* h, int off, int n);
+
+}  // namespace su2g
+
+namespace su2g {
+// Enqueue `ns` smearing steps on the handle's stream (no synchronisation).
+int ape_enqueue(su2g_lattice* h, int ns, double alpha, int mode);
+}  // namespace su2g

@@ -1,0 +1,474 @@
+// observables.cu -- plaquette, APE smearing, planar Wilson loops and the improved-clover charge.
+//
+// Reference routines: plaquette() (LGT_Code/modules/obs/plaquette.c:67-100), smearing_APE_*
+// (LGT_Code/modules/obs/smearing.c:42-168), compute_wloop / measureWilsonLoop
+// (LGT_Code/modules/obs/wilson.c:21-56, :268-324), topologicalCharge and helpers
+// (LGT_Code/modules/obs/topologicalcharge.c:18-199).
+//
+// Global sums are compensated FP64 (TwoSum) in every precision mode: per-thread sums, warp and
+// CTA trees, then a fixed-order pass over the per-CTA partials, so results are bit-reproducible
+// for a given lattice and grid.
+#include <algorithm>
+#include <cmath>
+
+#include "internal.cuh"
+
+using namespace su2g;
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// ------------------------------------------------------------ plaquette ---
+
+template <typename R>
+__global__ void __launch_bounds__(kBlock) k_plaquette(Field<R> U, Geom g, DD* __restrict__ partials)
+{
+    DD acc = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.V; i += gridDim.x * blockDim.x) {
+        const int par = i >= g.Vh, h = i - par * g.Vh, q = par ^ 1;
+        const Site s = site_of(g, par, h);
+        Q<R> u[4];
+        int xp[4];
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) {
+            u[mu] = U.ldh(mu, par, h);
+            xp[mu] = s.n + up_off_rt(g, s.c, mu);
+        }
+        double site = 0.0;
+#pragma unroll
+        for (int mu = 0; mu < 3; ++mu)
+#pragma unroll
+            for (int nu = mu + 1; nu < 4; ++nu) {
+                // Re tr U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag = 2 <U_mu(x)U_nu(x+mu), U_nu(x)U_mu(x+nu)>
+                Q<R> a = q_mul(u[mu], U.ld(nu, q, xp[mu]));
+                Q<R> b = q_mul(u[nu], U.ld(mu, q, xp[nu]));
+                site += (double)q_dot(a, b);
+            }
+        acc = dd_add(acc, site);
+    }
+    acc = dd_block_sum<kBlock>(acc);
+    if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+// ------------------------------------------------------------------- APE ---
+
+__host__ __device__ constexpr bool ape_updates(int mode, int mu)
+{
+    return mode == SU2G_APE_ALL ? true : (mode == SU2G_APE_SPATIAL ? mu != 0 : mu == 0);
+}
+// Is nu a staple direction for link mu?  staples_smearing(n, dir, dt) skips kk == dir and kk == dt
+// with dt = dir (all), 0 (spatial, temporal)  (smearing.c:51, :89, :122, :155).
+__host__ __device__ constexpr bool ape_staple(int mode, int mu, int nu)
+{
+    return nu != mu && (mode == SU2G_APE_ALL ? true : nu != 0);
+}
+
+// One Jacobi step U'_mu(x) = Proj(U_mu(x) + alpha S_mu(x)) with the staples of smearing.c:42-71:
+//   S_mu(x) = sum_nu U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag + U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu).
+// The middle product P = U_mu(x+nu) U_nu(x+mu)^dag of the forward staple of mu in plane nu is
+// also the dagger of the middle product of the forward staple of nu in plane mu, so each plane's
+// P is formed once.  Reads `in`, writes only the updated directions of `out`.
+template <typename R, int MODE>
+__global__ void __launch_bounds__(kBlock) k_ape(Field<R> in, Field<R> out, Geom g, R alpha)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.V; i += gridDim.x * blockDim.x) {
+        const int par = i >= g.Vh, h = i - par * g.Vh, q = par ^ 1;
+        const Site s = site_of(g, par, h);
+        Q<R> u[4], S[4];
+        int xp[4], xm[4];
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) {
+            xp[mu] = s.n + up_off_rt(g, s.c, mu);
+            xm[mu] = s.n + dn_off_rt(g, s.c, mu);
+            S[mu] = q_zero<R>();
+            bool need = ape_updates(MODE, mu);
+#pragma unroll
+            for (int nu = 0; nu < 4; ++nu) need = need || (ape_updates(MODE, nu) && ape_staple(MODE, nu, mu));
+            if (need) u[mu] = in.ldh(mu, par, h);
+        }
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu)
+#pragma unroll
+            for (int nu = mu + 1; nu < 4; ++nu) {
+                const bool a = ape_updates(MODE, mu) && ape_staple(MODE, mu, nu);
+                const bool b = ape_updates(MODE, nu) && ape_staple(MODE, nu, mu);
+                if (!a && !b) continue;
+                const Q<R> P = q_mul_nd(in.ld(mu, q, xp[nu]), in.ld(nu, q, xp[mu]));
+                if (a) S[mu] = q_add(S[mu], q_mul(u[nu], P));      // U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag
+                if (b) S[nu] = q_add(S[nu], q_mul_nd(u[mu], P));   // U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag
+            }
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) {
+            if (!ape_updates(MODE, mu)) continue;
+            const int dmu = xp[mu] - s.n;
+#pragma unroll
+            for (int nu = 0; nu < 4; ++nu) {
+                if (!ape_staple(MODE, mu, nu)) continue;
+                const Q<R> a = in.ld(nu, q, xm[nu]);          // U_nu(x-nu)
+                const Q<R> b = in.ld(mu, q, xm[nu]);          // U_mu(x-nu)
+                const Q<R> c = in.ld(nu, par, xm[nu] + dmu);  // U_nu(x-nu+mu)
+                S[mu] = q_add(S[mu], q_mul(q_mul_dn(a, b), c));
+            }
+            out.sth(mu, par, h, q_project(q_axpy(alpha, S[mu], u[mu])));
+        }
+    }
+}
+
+// ---------------------------------------------------------- Wilson loops ---
+
+constexpr int kWilsonTChunk = 32;   // T values one launch records
+constexpr int kWilsonWarps = kBlock / 32;
+
+template <int K>
+__device__ __forceinline__ int shift_k(const Geom& g, int ck, int j)
+{
+    int c = ck + j;
+    while (c >= g.L[K]) c -= g.L[K];
+    return (c - ck) * g.S[K];
+}
+
+__device__ __forceinline__ int shift_t(const Geom& g, int ct, int T)
+{
+    int c = ct + T;
+    while (c >= g.L[0]) c -= g.L[0];
+    return (c - ct) * g.S[0];
+}
+
+// For one site x and spatial direction K: all loops W(R, T) with R in [r0, r0+RC) and T in
+// [tlo, thi], by line products (compute_wloop, wilson.c:21-56, factored):
+//   W = (1/2) Re tr [T_T(x) S_R(x+T t) T_T(x+R k)^dag S_R(x)^dag] = <T_T(x) S_R(x+T t), S_R(x) T_T(x+R k)>
+// with T_T(y) = U_0(y) U_0(y+t) ... (T links) and S_R(y) = U_K(y) ... U_K(y+(R-1)k) (R links).
+// Temporal lines grow by one link per T; spatial lines at x+T t are rebuilt per T.
+template <typename R, int K, int RC>
+__device__ __forceinline__ void wilson_site(const Field<R>& U, const Geom& g, const Site& s, int par, int r0, int tlo,
+                                            int thi, DD* __restrict__ wacc)
+{
+    const int lane = threadIdx.x & 31;
+    Q<R> SX[RC], TR[RC];
+    int xr[RC];   // lexicographic index of x + (r0 + r) k
+    // spatial lines at x
+    Q<R> S = q_one<R>();
+    for (int j = 0; j < r0 - 1; ++j) S = q_mul(S, U.ld(K, par ^ (j & 1), s.n + shift_k<K>(g, s.c[K], j)));
+#pragma unroll
+    for (int r = 0; r < RC; ++r) {
+        const int j = r0 - 1 + r;
+        S = q_mul(S, U.ld(K, par ^ (j & 1), s.n + shift_k<K>(g, s.c[K], j)));
+        SX[r] = S;
+        xr[r] = s.n + shift_k<K>(g, s.c[K], j + 1);
+        TR[r] = q_one<R>();
+    }
+    Q<R> TX = q_one<R>();
+    for (int T = 1; T <= thi; ++T) {
+        const int tprev = shift_t(g, s.c[0], T - 1), tcur = shift_t(g, s.c[0], T);
+        const int pprev = par ^ ((T - 1) & 1);
+        TX = q_mul(TX, U.ld(0, pprev, s.n + tprev));
+#pragma unroll
+        for (int r = 0; r < RC; ++r) TR[r] = q_mul(TR[r], U.ld(0, pprev ^ ((r0 + r) & 1), xr[r] + tprev));
+        // spatial lines at x + T t
+        const int pT = par ^ (T & 1);
+        Q<R> ST = q_one<R>();
+        for (int j = 0; j < r0 - 1; ++j)
+            ST = q_mul(ST, U.ld(K, pT ^ (j & 1), s.n + tcur + shift_k<K>(g, s.c[K], j)));
+#pragma unroll
+        for (int r = 0; r < RC; ++r) {
+            const int j = r0 - 1 + r;
+            ST = q_mul(ST, U.ld(K, pT ^ (j & 1), s.n + tcur + shift_k<K>(g, s.c[K], j)));
+            double w = 0.0;
+            if (T >= tlo) w = (double)q_dot(q_mul(TX, ST), q_mul(SX[r], TR[r]));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+            if (T >= tlo && lane == 0) {
+                DD* slot = wacc + r * kWilsonTChunk + (T - tlo);
+                *slot = dd_add(*slot, w);
+            }
+        }
+    }
+}
+
+template <typename R, int RC>
+__global__ void __launch_bounds__(kBlock) k_wilson(Field<R> U, Geom g, int r0, int tlo, int thi,
+                                                   DD* __restrict__ partials)
+{
+    __shared__ DD wacc[kWilsonWarps][RC * kWilsonTChunk];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int j = lane; j < RC * kWilsonTChunk; j += 32) wacc[warp][j] = DD{0.0, 0.0};
+    __syncwarp();
+    // every lane of a warp runs the same number of iterations (shuffles inside)
+    const int stride = gridDim.x * blockDim.x;
+    const int base = blockIdx.x * blockDim.x + warp * 32;
+    for (int i0 = base; i0 < g.V; i0 += stride) {
+        const int i = i0 + lane;
+        const bool valid = i < g.V;
+        const int ii = valid ? i : i0;   // inactive lanes recompute a valid site and contribute 0
+        const int par = ii >= g.Vh, h = ii - par * g.Vh;
+        const Site s = site_of(g, par, h);
+        DD* acc = &wacc[warp][0];
+        // Lanes past the end recompute a valid site with an empty record window (tlo > thi), so
+        // that every lane takes part in the warp shuffles.
+        if (valid) {
+            wilson_site<R, 1, RC>(U, g, s, par, r0, tlo, thi, acc);
+            wilson_site<R, 2, RC>(U, g, s, par, r0, tlo, thi, acc);
+            wilson_site<R, 3, RC>(U, g, s, par, r0, tlo, thi, acc);
+        } else {
+            wilson_site<R, 1, RC>(U, g, s, par, r0, thi + 1, thi, acc);
+            wilson_site<R, 2, RC>(U, g, s, par, r0, thi + 1, thi, acc);
+            wilson_site<R, 3, RC>(U, g, s, par, r0, thi + 1, thi, acc);
+        }
+    }
+    __syncthreads();
+    // fixed-order sum over warps, one partial per slot
+    for (int j = threadIdx.x; j < RC * kWilsonTChunk; j += blockDim.x) {
+        DD v = {0.0, 0.0};
+        for (int w = 0; w < kWilsonWarps; ++w) v = dd_add(v, wacc[w][j]);
+        partials[(size_t)j * kMaxPartials + blockIdx.x] = v;
+    }
+}
+
+// --------------------------------------------------- topological charge ---
+
+// Walk `steps` links along direction D (negative: backwards), multiplying the path product.
+// Forward: acc *= U_D(y), y += D.  Backward: y -= D, acc *= U_D(y)^dag  (computeLine,
+// topologicalcharge.c:18-44).
+template <typename R, int D>
+__device__ __forceinline__ void walk(const Field<R>& U, const Geom& g, int& n, int& c, int& par, int steps, Q<R>& acc)
+{
+    if (steps > 0) {
+        for (int i = 0; i < steps; ++i) {
+            acc = q_mul(acc, U.ld(D, par, n));
+            if (c == g.L[D] - 1) { n -= (g.L[D] - 1) * g.S[D]; c = 0; }
+            else { n += g.S[D]; ++c; }
+            par ^= 1;
+        }
+    } else {
+        for (int i = 0; i < -steps; ++i) {
+            if (c == 0) { n += (g.L[D] - 1) * g.S[D]; c = g.L[D] - 1; }
+            else { n -= g.S[D]; --c; }
+            par ^= 1;
+            acc = q_mul_nd(acc, U.ld(D, par, n));
+        }
+    }
+}
+
+// Improved clover field strength in plane (A, B) at site s:
+// F = [(k1 C1 + k2 C2 + k3 C3) - h.c.]/2 with C_e = (1/4) sum of the four e x e leaves and
+// (k1, k2, k3) = (1.5, -0.15, 1/90)  (computeCloverAverages / computeCloverProducts /
+// hermitianTraceless, topologicalcharge.c:46-162).  The leaves, all starting and ending at x:
+//   +A +B -A -B,   -B +A +B -A,   +B -A -B +A,   -A -B +A +B.
+template <typename R, int A, int B>
+__device__ __forceinline__ Q<R> clover_F(const Field<R>& U, const Geom& g, const Site& s, int par)
+{
+    const R kcoef[3] = {R(1.5), R(-0.15), R(1.0 / 90.0)};
+    Q<R> F = q_zero<R>();
+#pragma unroll
+    for (int e = 1; e <= 3; ++e) {
+        Q<R> C = q_zero<R>();
+        int n = s.n, ca = s.c[A], cb = s.c[B], p = par;
+        Q<R> l = q_one<R>();
+        walk<R, A>(U, g, n, ca, p, e, l); walk<R, B>(U, g, n, cb, p, e, l);
+        walk<R, A>(U, g, n, ca, p, -e, l); walk<R, B>(U, g, n, cb, p, -e, l);
+        C = q_add(C, l);
+        l = q_one<R>();
+        walk<R, B>(U, g, n, cb, p, -e, l); walk<R, A>(U, g, n, ca, p, e, l);
+        walk<R, B>(U, g, n, cb, p, e, l); walk<R, A>(U, g, n, ca, p, -e, l);
+        C = q_add(C, l);
+        l = q_one<R>();
+        walk<R, B>(U, g, n, cb, p, e, l); walk<R, A>(U, g, n, ca, p, -e, l);
+        walk<R, B>(U, g, n, cb, p, -e, l); walk<R, A>(U, g, n, ca, p, e, l);
+        C = q_add(C, l);
+        l = q_one<R>();
+        walk<R, A>(U, g, n, ca, p, -e, l); walk<R, B>(U, g, n, cb, p, -e, l);
+        walk<R, A>(U, g, n, ca, p, e, l); walk<R, B>(U, g, n, cb, p, e, l);
+        C = q_add(C, l);
+        F = q_axpy(kcoef[e - 1] * R(0.25), C, F);
+    }
+    F.c0 = R(0);   // (F - F^dag)/2 keeps the su(2) part
+    return F;
+}
+
+// q(x) = 8 [tr F01 F23 + tr F02 F31 + tr F03 F12], tr = 2 c0 (topologicalcharge.c:175-178)
+template <typename R>
+__device__ __forceinline__ double qtop_density(const Field<R>& U, const Geom& g, const Site& s, int par)
+{
+    double d = 0.0;
+    d += 16.0 * (double)q_mul(clover_F<R, 0, 1>(U, g, s, par), clover_F<R, 2, 3>(U, g, s, par)).c0;
+    d += 16.0 * (double)q_mul(clover_F<R, 0, 2>(U, g, s, par), clover_F<R, 3, 1>(U, g, s, par)).c0;
+    d += 16.0 * (double)q_mul(clover_F<R, 0, 3>(U, g, s, par), clover_F<R, 1, 2>(U, g, s, par)).c0;
+    return d;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBlock) k_qtop(Field<R> U, Geom g, DD* __restrict__ partials)
+{
+    DD acc = {0.0, 0.0}, aabs = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.V; i += gridDim.x * blockDim.x) {
+        const int par = i >= g.Vh, h = i - par * g.Vh;
+        const Site s = site_of(g, par, h);
+        const double d = qtop_density<R>(U, g, s, par);
+        acc = dd_add(acc, d);
+        aabs = dd_add(aabs, fabs(d));
+    }
+    acc = dd_block_sum<kBlock>(acc);
+    aabs = dd_block_sum<kBlock>(aabs);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = acc;
+        partials[kMaxPartials + blockIdx.x] = aabs;
+    }
+}
+
+int ensure_alt(su2g_lattice* h)
+{
+    if (h->field_alt) return SU2G_OK;
+    cudaError_t e = cudaMalloc(&h->field_alt, 4ull * h->g.V * h->link_bytes);
+    if (e != cudaSuccess) return check_cuda(h, e, "allocating the smearing field");
+    // the partner of each direction is the slot in the other allocation not currently used
+    for (int mu = 0; mu < 4; ++mu) {
+        size_t off = (size_t)mu * 2 * h->g.Vh * h->link_bytes;
+        h->altp[mu] = (char*)h->field_alt + off;
+    }
+    return SU2G_OK;
+}
+
+template <typename R>
+void launch_ape(su2g_lattice* h, int mode, R alpha, int grid)
+{
+    Field<R> in = make_field<R>(h->dirp, h->g.Vh), out = make_field<R>(h->altp, h->g.Vh);
+    if (mode == SU2G_APE_ALL) k_ape<R, SU2G_APE_ALL><<<grid, kBlock, 0, h->stream>>>(in, out, h->g, alpha);
+    else if (mode == SU2G_APE_SPATIAL) k_ape<R, SU2G_APE_SPATIAL><<<grid, kBlock, 0, h->stream>>>(in, out, h->g, alpha);
+    else k_ape<R, SU2G_APE_TEMPORAL><<<grid, kBlock, 0, h->stream>>>(in, out, h->g, alpha);
+}
+
+template <typename R, int RC>
+void launch_wilson_t(su2g_lattice* h, int r0, int tlo, int thi, int grid)
+{
+    k_wilson<R, RC><<<grid, kBlock, 0, h->stream>>>(make_field<R>(h->dirp, h->g.Vh), h->g, r0, tlo, thi, h->partials);
+}
+
+template <typename R>
+void launch_wilson(su2g_lattice* h, int rc, int r0, int tlo, int thi, int grid)
+{
+    switch (rc) {
+        case 1: launch_wilson_t<R, 1>(h, r0, tlo, thi, grid); break;
+        case 2: launch_wilson_t<R, 2>(h, r0, tlo, thi, grid); break;
+        case 4: launch_wilson_t<R, 4>(h, r0, tlo, thi, grid); break;
+        default: launch_wilson_t<R, 8>(h, r0, tlo, thi, grid); break;
+    }
+}
+
+}  // namespace
+
+extern "C" int su2g_plaquette(su2g_lattice* h, double* p)
+{
+    if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_plaquette: null handle");
+    if (!p) return set_error(h, SU2G_EINVAL, "su2g_plaquette: null output");
+    cudaSetDevice(h->device);
+    const int grid = grid_for(h, h->g.V, 8);
+    launch_begin(h, SU2G_K_PLAQUETTE);
+    if (h->prec == SU2G_FP32)
+        k_plaquette<float><<<grid, kBlock, 0, h->stream>>>(make_field<float>(h->dirp, h->g.Vh), h->g, h->partials);
+    else
+        k_plaquette<double><<<grid, kBlock, 0, h->stream>>>(make_field<double>(h->dirp, h->g.Vh), h->g, h->partials);
+    int rc = launch_end(h, SU2G_K_PLAQUETTE, "plaquette kernel");
+    // plaq = sum 2 c0 / (2 * 6 * V)  (plaquette.c:97); the kernel sums c0 = (1/2) Re tr
+    if (!rc) rc = finalize(h, grid, 1, 1.0 / (6.0 * (double)h->g.V), 0);
+    if (!rc) rc = fetch_results(h, 0, 1);
+    if (!rc) *p = h->h_out[0];
+    return rc;
+}
+
+// Enqueue `ns` smearing steps without synchronising (used by su2g_ape and the adjoint).
+int su2g::ape_enqueue(su2g_lattice* h, int ns, double alpha, int mode)
+{
+    int rc = ensure_alt(h);
+    if (rc) return rc;
+    const int grid = grid_for(h, h->g.V, 8);
+    for (int step = 0; step < ns; ++step) {
+        launch_begin(h, SU2G_K_APE);
+        if (h->prec == SU2G_FP32) launch_ape<float>(h, mode, (float)alpha, grid);
+        else launch_ape<double>(h, mode, alpha, grid);
+        if ((rc = launch_end(h, SU2G_K_APE, "APE kernel"))) return rc;
+        for (int mu = 0; mu < 4; ++mu)
+            if (ape_updates(mode, mu)) std::swap(h->dirp[mu], h->altp[mu]);
+    }
+    return SU2G_OK;
+}
+
+extern "C" int su2g_ape(su2g_lattice* h, int32_t ns, double alpha, int32_t mode)
+{
+    if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_ape: null handle");
+    if (ns < 0 || mode < SU2G_APE_ALL || mode > SU2G_APE_TEMPORAL || !std::isfinite(alpha))
+        return set_error(h, SU2G_EINVAL, "su2g_ape: bad argument (ns=%d, mode=%d)", ns, mode);
+    cudaSetDevice(h->device);
+    return ape_enqueue(h, ns, alpha, mode);
+}
+
+extern "C" int su2g_wilson(su2g_lattice* h, const int32_t* R, const int32_t* T, int32_t n, double* w)
+{
+    if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_wilson: null handle");
+    if (n < 0 || (n > 0 && (!R || !T || !w))) return set_error(h, SU2G_EINVAL, "su2g_wilson: bad argument");
+    if (n == 0) return SU2G_OK;
+    int rmax = 0, tmax = 0;
+    for (int i = 0; i < n; ++i) {
+        if (R[i] < 1 || T[i] < 1) return set_error(h, SU2G_EINVAL, "su2g_wilson: R and T must be >= 1");
+        rmax = std::max(rmax, (int)R[i]);
+        tmax = std::max(tmax, (int)T[i]);
+    }
+    // measureWilsonLoop refuses T > L_t - 1 (wilson.c:290-291)
+    if (tmax > h->g.L[0] - 1)
+        return set_error(h, SU2G_EINVAL, "su2g_wilson: lattice too small to measure loops (T=%d, L_t=%d)", tmax,
+                         h->g.L[0]);
+    cudaSetDevice(h->device);
+    int rc = ensure_partials(h, 8 * kWilsonTChunk);
+    if (rc) return rc;
+    const int grid = grid_for(h, h->g.V, 4);
+    std::vector<double> grid_w((size_t)rmax * tmax, 0.0);
+    std::vector<char> want((size_t)rmax * tmax, 0);
+    for (int i = 0; i < n; ++i) want[(size_t)(R[i] - 1) * tmax + (T[i] - 1)] = 1;
+    // R in chunks of 8/4/2/1, T in chunks of kWilsonTChunk; a chunk with no wanted pair is skipped
+    for (int r0 = 1; r0 <= rmax;) {
+        int left = rmax - r0 + 1, rc_n = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
+        for (int tlo = 1; tlo <= tmax; tlo += kWilsonTChunk) {
+            int thi = std::min(tmax, tlo + kWilsonTChunk - 1);
+            bool any = false;
+            for (int r = r0; r < r0 + rc_n; ++r)
+                for (int t = tlo; t <= thi; ++t) any = any || want[(size_t)(r - 1) * tmax + (t - 1)];
+            if (!any) continue;
+            launch_begin(h, SU2G_K_WILSON);
+            if (h->prec == SU2G_FP32) launch_wilson<float>(h, rc_n, r0, tlo, thi, grid);
+            else launch_wilson<double>(h, rc_n, r0, tlo, thi, grid);
+            if ((rc = launch_end(h, SU2G_K_WILSON, "Wilson loop kernel"))) return rc;
+            const int nslots = rc_n * kWilsonTChunk;
+            // W = sum_x,k c0 / (3 V)  (wilson.c:322: sum of Re tr / (3 V 2))
+            if ((rc = finalize(h, grid, nslots, 1.0 / (3.0 * (double)h->g.V), 0))) return rc;
+            if ((rc = fetch_results(h, 0, nslots))) return rc;
+            for (int r = 0; r < rc_n; ++r)
+                for (int t = tlo; t <= thi; ++t)
+                    grid_w[(size_t)(r0 + r - 1) * tmax + (t - 1)] = h->h_out[r * kWilsonTChunk + (t - tlo)];
+        }
+        r0 += rc_n;
+    }
+    for (int i = 0; i < n; ++i) w[i] = grid_w[(size_t)(R[i] - 1) * tmax + (T[i] - 1)];
+    return SU2G_OK;
+}
+
+extern "C" int su2g_qtop(su2g_lattice* h, double* q, double* sum_abs)
+{
+    if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_qtop: null handle");
+    if (!q) return set_error(h, SU2G_EINVAL, "su2g_qtop: null output");
+    cudaSetDevice(h->device);
+    const int grid = grid_for(h, h->g.V, 4);
+    launch_begin(h, SU2G_K_QTOP);
+    if (h->prec == SU2G_FP32)
+        k_qtop<float><<<grid, kBlock, 0, h->stream>>>(make_field<float>(h->dirp, h->g.Vh), h->g, h->partials);
+    else
+        k_qtop<double><<<grid, kBlock, 0, h->stream>>>(make_field<double>(h->dirp, h->g.Vh), h->g, h->partials);
+    int rc = launch_end(h, SU2G_K_QTOP, "topological charge kernel");
+    // Q = sum_x q(x) / (32 pi^2)  (topologicalcharge.c:194)
+    if (!rc) rc = finalize(h, grid, 2, 1.0 / (32.0 * kPi * kPi), 0);
+    if (!rc) rc = fetch_results(h, 0, 2);
+    if (!rc) {
+        *q = h->h_out[0];
+        if (sum_abs) *sum_abs = h->h_out[1];
+    }
+    return rc;
+}

@@ -1,0 +1,263 @@
+"""ctypes binding of libsu2g.so (include/su2g.h).
+
+This is a thin host-side convenience layer over the C ABI for tests, benchmarks and Python
+callers; the C ABI itself is the product boundary.  Every call goes to the CUDA library; if
+the library cannot be loaded or no sm_100 GPU is present, the calls raise -- there is no CPU
+fallback.
+"""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from . import build as _build
+
+FP32, FP64 = 0, 1
+START = {"cold": 0, "haar": 1, "ref": 2}
+APE = {"all": 0, "spatial": 1, "temporal": 2}
+HEATBATH, OVERRELAX = 0, 1
+KERNEL_CLASSES = ["heatbath", "overrelax", "plaquette", "ape", "wilson", "qtop", "reduce", "other"]
+
+_HEADER = os.path.join(_build.REPO, "include", "su2g.h")
+
+
+class Su2gError(RuntimeError):
+    """A libsu2g call returned a non-zero status."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"su2g error {code}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("dims", ctypes.c_int32 * 4),
+        ("precision", ctypes.c_int32),
+        ("start", ctypes.c_int32),
+        ("beta", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+        ("replica", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+_lib = None
+_P = ctypes.c_void_p
+_DP = ctypes.POINTER(ctypes.c_double)
+_I32P = ctypes.POINTER(ctypes.c_int32)
+_I64P = ctypes.POINTER(ctypes.c_int64)
+
+_SIGS = {
+    "su2g_create": (ctypes.c_int, [ctypes.POINTER(Params), ctypes.POINTER(_P)]),
+    "su2g_destroy": (ctypes.c_int, [_P]),
+    "su2g_last_error": (ctypes.c_char_p, [_P]),
+    "su2g_start": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_uint64]),
+    "su2g_info": (ctypes.c_int, [_P, _I32P, _I32P, _I64P, ctypes.POINTER(ctypes.c_uint32)]),
+    "su2g_set_beta": (ctypes.c_int, [_P, ctypes.c_double]),
+    "su2g_set_sweep_counter": (ctypes.c_int, [_P, ctypes.c_uint32]),
+    "su2g_upload_aos_f64": (ctypes.c_int, [_P, _DP]),
+    "su2g_download_aos_f64": (ctypes.c_int, [_P, _DP]),
+    "su2g_sweep": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP]),
+    "su2g_update_pass": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]),
+    "su2g_plaquette": (ctypes.c_int, [_P, _DP]),
+    "su2g_ape": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32]),
+    "su2g_wilson": (ctypes.c_int, [_P, _I32P, _I32P, ctypes.c_int32, _DP]),
+    "su2g_qtop": (ctypes.c_int, [_P, _DP, _DP]),
+    "su2g_kp_histogram": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32, _I64P]),
+    "su2g_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_P)]),
+    "su2g_host_free": (ctypes.c_int, [_P]),
+    "su2g_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+    "su2g_synchronize": (ctypes.c_int, [_P]),
+    "su2g_timer_begin": (ctypes.c_int, [_P]),
+    "su2g_timer_end": (ctypes.c_int, [_P, _DP]),
+    "su2g_profile_enable": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "su2g_profile_read": (ctypes.c_int, [_P, ctypes.c_int32, _I64P, _DP]),
+}
+
+
+def header_functions(path=_HEADER):
+    """Names of every function declared in include/su2g.h."""
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(su2g_[a-z0-9_]+)\s*\(", text)))
+
+
+def load(path=None, build_if_missing=True):
+    """Load libsu2g.so (building it with nvcc if it is missing or stale)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if path is None:
+        path = _build.build() if build_if_missing else _build.LIB
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _as_dp(a):
+    return a.ctypes.data_as(_DP)
+
+
+class PinnedArray:
+    """A numpy array over page-locked host memory from su2g_host_alloc."""
+
+    def __init__(self, shape, dtype=np.float64):
+        self.lib = load()
+        nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        p = _P()
+        rc = self.lib.su2g_host_alloc(nbytes, ctypes.byref(p))
+        if rc != 0:
+            raise Su2gError(rc, self.lib.su2g_last_error(None).decode())
+        self.ptr = p
+        buf = (ctypes.c_char * nbytes).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def free(self):
+        if getattr(self, "ptr", None):
+            self.array = None
+            self.lib.su2g_host_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Lattice:
+    """One SU(2) gauge field resident on a B200, driven through the C ABI."""
+
+    def __init__(self, dims, precision="fp32", beta=2.3, seed=1, start="cold", replica=0, device=0):
+        self.lib = load()
+        p = Params()
+        for i in range(4):
+            p.dims[i] = int(dims[i])
+        p.precision = FP64 if str(precision).lower() in ("fp64", "f64", "double", "1") else FP32
+        p.start = START[start] if isinstance(start, str) else int(start)
+        p.beta = float(beta)
+        p.seed = int(seed)
+        p.replica = int(replica)
+        p.device = int(device)
+        h = _P()
+        rc = self.lib.su2g_create(ctypes.byref(p), ctypes.byref(h))
+        if rc != 0:
+            raise Su2gError(rc, self.lib.su2g_last_error(None).decode())
+        self.h = h
+        self.dims = tuple(int(d) for d in dims)
+        self.volume = int(np.prod(self.dims))
+        self.precision = "fp64" if p.precision == FP64 else "fp32"
+
+    # -- plumbing
+    def _check(self, rc):
+        if rc != 0:
+            raise Su2gError(rc, self.lib.su2g_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.su2g_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state
+    def start(self, mode="cold", seed=1):
+        self._check(self.lib.su2g_start(self.h, START[mode] if isinstance(mode, str) else int(mode), int(seed)))
+
+    def info(self):
+        dims = (ctypes.c_int32 * 4)()
+        prec, vol, sw = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_uint32()
+        self._check(self.lib.su2g_info(self.h, dims, ctypes.byref(prec), ctypes.byref(vol), ctypes.byref(sw)))
+        return {"dims": tuple(dims), "precision": prec.value, "volume": vol.value, "hb_sweeps": sw.value}
+
+    def set_beta(self, beta):
+        self._check(self.lib.su2g_set_beta(self.h, float(beta)))
+
+    def set_sweep_counter(self, n):
+        self._check(self.lib.su2g_set_sweep_counter(self.h, int(n)))
+
+    def upload(self, links):
+        a = np.ascontiguousarray(links, dtype=np.float64).reshape(self.volume * 16)
+        self._check(self.lib.su2g_upload_aos_f64(self.h, _as_dp(a)))
+
+    def download(self, out=None):
+        a = out if out is not None else np.empty((self.volume, 4, 4), dtype=np.float64)
+        self._check(self.lib.su2g_download_aos_f64(self.h, _as_dp(a)))
+        return a
+
+    # -- updates
+    def sweep(self, n_sweeps=1, n_hb=1, n_or=0, acc=False):
+        if acc:
+            v = ctypes.c_double()
+            self._check(self.lib.su2g_sweep(self.h, n_sweeps, n_hb, n_or, ctypes.byref(v)))
+            return v.value
+        self._check(self.lib.su2g_sweep(self.h, n_sweeps, n_hb, n_or, None))
+        return None
+
+    def update_pass(self, kind, mu, parity, sweep=0):
+        self._check(self.lib.su2g_update_pass(self.h, int(kind), int(mu), int(parity), int(sweep)))
+
+    # -- observables
+    def plaquette(self):
+        v = ctypes.c_double()
+        self._check(self.lib.su2g_plaquette(self.h, ctypes.byref(v)))
+        return v.value
+
+    def ape(self, ns, alpha, mode="all"):
+        self._check(self.lib.su2g_ape(self.h, int(ns), float(alpha), APE[mode] if isinstance(mode, str) else int(mode)))
+
+    def wilson(self, R, T):
+        R = np.ascontiguousarray(R, dtype=np.int32)
+        T = np.ascontiguousarray(T, dtype=np.int32)
+        w = np.empty(len(R), dtype=np.float64)
+        self._check(self.lib.su2g_wilson(self.h, R.ctypes.data_as(_I32P), T.ctypes.data_as(_I32P), len(R), _as_dp(w)))
+        return w
+
+    def qtop(self, with_abs=False):
+        q, a = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.su2g_qtop(self.h, ctypes.byref(q), ctypes.byref(a)))
+        return (q.value, a.value) if with_abs else q.value
+
+    def kp_histogram(self, alpha, seed, n, nbins=200):
+        c = np.zeros(nbins, dtype=np.int64)
+        self._check(self.lib.su2g_kp_histogram(self.h, float(alpha), int(seed), int(n), int(nbins),
+                                               c.ctypes.data_as(_I64P)))
+        return c
+
+    # -- timing
+    def synchronize(self):
+        self._check(self.lib.su2g_synchronize(self.h))
+
+    def timer_begin(self):
+        self._check(self.lib.su2g_timer_begin(self.h))
+
+    def timer_end(self):
+        v = ctypes.c_double()
+        self._check(self.lib.su2g_timer_end(self.h, ctypes.byref(v)))
+        return v.value
+
+    def profile(self, enable=True):
+        self._check(self.lib.su2g_profile_enable(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        out = {}
+        for i, name in enumerate(KERNEL_CLASSES):
+            n, ms = ctypes.c_int64(), ctypes.c_double()
+            self._check(self.lib.su2g_profile_read(self.h, i, ctypes.byref(n), ctypes.byref(ms)))
+            out[name] = (n.value, ms.value)
+        return out

@@ -1,0 +1,117 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures under tests/golden/ from the reference's own C code.
+
+This script is the provenance of every file next to it.  It needs the reference
+tree (default /root/reference, override with SU2_REFERENCE_ROOT) and gcc; it
+compiles the reference from its sources with oracle/build_ref.sh and runs the
+resulting harness binaries (oracle/ref_harness.c).  The GPU box has no
+reference tree, which is why the outputs are committed.
+
+Outputs
+  cfg_*.cfg      configurations in the reference's binary format
+                 (LGT_Code/modules/io/config_IO.c:40-117): written by the
+                 reference's writeConfig after its own heatbath chain, APE
+                 smearing or Philox-injected heatbath sweeps.
+  golden.json    observables computed by the reference's own routines
+                 (%.17g): plaquette, APE, W(R,T), Q, injected-heatbath
+                 acceptance and plaquette.
+  kp_improved.dat  the reference's Kennedy-Pendleton sampler histogram at
+                 alpha=7 (copied from LGT_Code/main_test/improved.dat; 200 bins
+                 of N=1e8 draws; column 2 is count*200/N).
+"""
+import json
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("SU2_REFERENCE_ROOT", "/root/reference")
+
+LATTICES = {
+    # dims T,X,Y,Z : (start, seed, beta, sweeps)
+    "4x4x4x4": (1, 3, 2.3, 5),
+    "6x4x4x8": (1, 5, 3.09, 10),
+    "8x8x8x8": (0, 1, 3.09, 50),
+}
+LINK_LEVEL = {"4x4x4x4", "6x4x4x8"}  # small enough to commit smeared / updated fields
+
+
+def harness(dims, inj=False):
+    return os.path.join(REPO, "oracle", "_ref", dims, "harness_inj" if inj else "harness")
+
+
+def run(cmd):
+    out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
+    res = []
+    for line in out.splitlines():
+        if line.startswith("RESULT "):
+            res.append(line.split()[2:])
+    return res
+
+
+def main():
+    subprocess.run([os.path.join(REPO, "oracle", "build_ref.sh"), REF] + list(LATTICES), check=True)
+    gold = {"reference": "daggerfall247/Masterarbeit LGT_Code, compiled by oracle/build_ref.sh", "lattices": {}}
+    for dims, (start, seed, beta, nsw) in LATTICES.items():
+        d = [int(x) for x in dims.split("x")]
+        base = f"cfg_{dims}_base.cfg"
+        r = run([harness(dims), "gen", str(start), str(seed), str(beta), str(nsw), os.path.join(HERE, base)])
+        entry = {
+            "dims": d,
+            "base": base,
+            "gen": {"start": start, "seed": seed, "beta": beta, "sweeps": nsw,
+                    "plaq_trace": [float(x[1]) for x in r]},
+        }
+        entry["plaq"] = float(run([harness(dims), "plaq", os.path.join(HERE, base)])[0][0])
+
+        # APE smearing, three modes (smearing.c:74-168)
+        entry["ape"] = {}
+        for mode in ("all", "spatial", "temporal"):
+            ns, alpha = 3, 0.5
+            out = os.path.join(HERE if dims in LINK_LEVEL else "/tmp", f"cfg_{dims}_ape_{mode}.cfg")
+            rr = run([harness(dims), "ape", os.path.join(HERE, base), mode, str(ns), str(alpha), out])
+            e = {"ns": ns, "alpha": alpha, "plaq": float(rr[0][0])}
+            if dims in LINK_LEVEL:
+                e["cfg"] = os.path.basename(out)
+            entry["ape"][mode] = e
+
+        # Wilson loops, explicit list mode (wilson.c:268-324)
+        lt = d[0]
+        R = [r_ for r_ in range(1, 7) for t_ in range(1, lt)]
+        T = [t_ for r_ in range(1, 7) for t_ in range(1, lt)]
+        rr = run([harness(dims), "wil", os.path.join(HERE, base), ",".join(map(str, R)), ",".join(map(str, T))])
+        entry["wilson"] = [[int(x[0]), int(x[1]), float(x[2])] for x in rr]
+
+        # Topological charge after cumulative APE_all steps (qtop.c:76-91)
+        for alpha, Ns in ((0.1, [0, 1, 5]), (0.5, [0, 3])):
+            rr = run([harness(dims), "qtop", os.path.join(HERE, base), str(alpha), ",".join(map(str, Ns))])
+            entry.setdefault("qtop", []).append({"alpha": alpha, "N": Ns, "Q": [float(x[1]) for x in rr]})
+
+        # Reference heatbath on injected Philox uniforms, checkerboard order
+        hb_seed, hb_beta, sweep0, nhb = 12345, 3.09, 7, 2
+        out = os.path.join(HERE if dims in LINK_LEVEL else "/tmp", f"cfg_{dims}_hbinj.cfg")
+        rr = run([harness(dims, True), "hbinj", os.path.join(HERE, base), str(hb_seed), str(hb_beta), str(sweep0),
+                  str(nhb), out])
+        e = {"seed": hb_seed, "beta": hb_beta, "sweep0": sweep0, "sweeps": nhb,
+             "acc": [float(x[1]) for x in rr], "plaq": [float(x[2]) for x in rr]}
+        if dims in LINK_LEVEL:
+            e["cfg"] = os.path.basename(out)
+        entry["hbinj"] = e
+
+        # Hot start of initGaugeField on injected Philox uniforms
+        if dims in LINK_LEVEL:
+            out = os.path.join(HERE, f"cfg_{dims}_hotinj.cfg")
+            rr = run([harness(dims, True), "hotinj", "99", out])
+            entry["hotinj"] = {"seed": 99, "plaq": float(rr[0][0]), "cfg": os.path.basename(out)}
+        gold["lattices"][dims] = entry
+
+    shutil.copyfile(os.path.join(REF, "LGT_Code", "main_test", "improved.dat"), os.path.join(HERE, "kp_improved.dat"))
+    with open(os.path.join(HERE, "golden.json"), "w") as f:
+        json.dump(gold, f, indent=1)
+    print("wrote", os.path.join(HERE, "golden.json"))
+
+
+if __name__ == "__main__":
+    sys.exit(main())
