@@ -72,7 +72,9 @@ __host__ __device__ constexpr bool ape_staple(int mode, int mu, int nu)
 template <typename R, int MODE>
 __global__ void __launch_bounds__(kBlock) k_ape(Field<R> in, Field<R> out, Geom g, R alpha)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.V; i += gridDim.x * blockDim.x) {
+    // one site per thread, CTAs dispatched in order (a contiguous window of sites is in flight)
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < g.V) {
         const int par = i >= g.Vh, h = i - par * g.Vh, q = par ^ 1;
         const Site s = site_of(g, par, h);
         Q<R> u[4], S[4];
@@ -381,7 +383,7 @@ int su2g::ape_enqueue(su2g_lattice* h, int ns, double alpha, int mode)
 {
     int rc = ensure_alt(h);
     if (rc) return rc;
-    const int grid = grid_for(h, h->g.V, 8);
+    const int grid = (int)((h->g.V + kBlock - 1) / kBlock);
     for (int step = 0; step < ns; ++step) {
         launch_begin(h, SU2G_K_APE);
         if (h->prec == SU2G_FP32) launch_ape<float>(h, mode, (float)alpha, grid);

@@ -32,26 +32,32 @@ __device__ __forceinline__ double log_r(double x) { return log(x); }
 
 // Staple sum A with U_mu(x) A = sum of the six plaquettes containing U_mu(x)  (metro.c:34-63):
 //   A = sum_{nu != mu} U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag + U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu)
+// All 18 links are loaded before the first product, so that a thread keeps every load of its
+// staple in flight at once (the pass is bound by memory latency x parallelism, not by ALU).
 template <typename R, int MU>
 __device__ __forceinline__ Q<R> staple_update(const Field<R>& U, const Geom& g, const Site& s, int par)
 {
     const int q = par ^ 1;
     const int dmu = up_off<MU>(g, s);
     const int xmu = s.n + dmu;
-    Q<R> A = q_zero<R>();
+    Q<R> a[3], b[3], c[3], d[3], e[3], f[3];
 #pragma unroll
-    for (int nu = 0; nu < 4; ++nu) {
-        if (nu == MU) continue;
+    for (int k = 0; k < 3; ++k) {
+        const int nu = k < MU ? k : k + 1;
         const int xnu = s.n + up_off_rt(g, s.c, nu);
         const int xmn = s.n + dn_off_rt(g, s.c, nu);
-        Q<R> a = U.ld(nu, q, xmu);           // U_nu(x+mu)
-        Q<R> b = U.ld(MU, q, xnu);           // U_mu(x+nu)
-        Q<R> c = U.ld(nu, par, s.n);         // U_nu(x)
-        A = q_add(A, q_mul_nd(q_mul_nd(a, b), c));
-        Q<R> d = U.ld(nu, par, xmn + dmu);   // U_nu(x-nu+mu)
-        Q<R> e = U.ld(MU, q, xmn);           // U_mu(x-nu)
-        Q<R> f = U.ld(nu, q, xmn);           // U_nu(x-nu)
-        A = q_add(A, q_mul_dn(q_mul(e, d), f));
+        a[k] = U.ld(nu, q, xmu);           // U_nu(x+mu)
+        b[k] = U.ld(MU, q, xnu);           // U_mu(x+nu)
+        c[k] = U.ld(nu, par, s.n);         // U_nu(x)
+        d[k] = U.ld(nu, par, xmn + dmu);   // U_nu(x-nu+mu)
+        e[k] = U.ld(MU, q, xmn);           // U_mu(x-nu)
+        f[k] = U.ld(nu, q, xmn);           // U_nu(x-nu)
+    }
+    Q<R> A = q_zero<R>();
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        A = q_add(A, q_mul_nd(q_mul_nd(a[k], b[k]), c[k]));
+        A = q_add(A, q_mul_dn(q_mul(e[k], d[k]), f[k]));
     }
     return A;
 }
@@ -76,17 +82,19 @@ __device__ __forceinline__ Q<R> fallback_link(R r0, R r1, R r2)
 }
 
 // Kennedy-Pendleton heatbath of one link given its staple sum (heatbath.c:76-149).
-// Returns the new link; `acc` receives 1/trials (0 for the zero-staple fallback).
+// Writes the new link to `out`; `acc` receives 1/trials (0 for the zero-staple fallback).  Returns
+// false only if the trial bound is hit (the link then keeps its old value).
 template <typename R>
-__device__ __forceinline__ Q<R> heatbath_link(const Q<R>& A, const Q<R>& old, R beta, uint64_t seed, uint32_t site,
-                                              uint32_t sweep, uint32_t mu, uint32_t replica, double& acc,
+__device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t seed, uint32_t site, uint32_t sweep,
+                                              uint32_t mu, uint32_t replica, double& acc, Q<R>& out,
                                               unsigned* status)
 {
     const R k = sqrt_r(q_norm2(A));
     if (!(k > eps_r<R>())) {
         U4 w = link_random(seed, site, sweep, mu, 1u, 1u, kStreamUpdate, replica);
         acc = 0.0;
-        return fallback_link<R>(u01(w.x, R(0)), u01(w.y, R(0)), u01(w.z, R(0)));
+        out = fallback_link<R>(u01(w.x, R(0)), u01(w.y, R(0)), u01(w.z, R(0)));
+        return true;
     }
     const R ik = R(1) / k;
     const R ia = R(1) / (k * beta);          // 1/alpha, alpha = k*beta (heatbath.c:142)
@@ -100,10 +108,10 @@ __device__ __forceinline__ Q<R> heatbath_link(const Q<R>& A, const Q<R>& old, R 
         // X1 = -ln(u0)/alpha, X2 = -ln(u1)/alpha, delta = X2 + X1 cos^2(2 pi u2)  (heatbath.c:86-90)
         delta = -(log_r(u1) + log_r(u0) * (c * c)) * ia;
         if (u3 * u3 <= R(1) - R(0.5) * delta) break;   // heatbath.c:94
-        if (trial >= kMaxTrials) {
+        if (trial >= kMaxTrials) {   // the link keeps its value and the host sees the status bit
             atomicOr(status, kStatusKpTrials);
             acc = 0.0;
-            return old;
+            return false;
         }
     }
     acc = 1.0 / (double)trial;
@@ -117,7 +125,8 @@ __device__ __forceinline__ Q<R> heatbath_link(const Q<R>& A, const Q<R>& old, R 
     const R len = sqrt_r(delta * (R(2) - delta));          // sqrt(1 - (1-delta)^2)
     Q<R> X = q_make<R>(R(1) - delta, len * sth * cph, len * sth * sph, len * cth);
     // U = X V^dag, V = A/k  (heatbath.c:140-146)
-    return q_mul_nd(X, q_scale(A, ik));
+    out = q_mul_nd(X, q_scale(A, ik));
+    return true;
 }
 
 // Overrelaxation U' = (W U W)^dag with W = A/|A|: keeps Re tr(U A), and applied twice is the identity.
@@ -135,20 +144,20 @@ __global__ void __launch_bounds__(kBlock) k_update(Field<R> U, Geom g, int par, 
                                                    uint32_t replica, double* __restrict__ acc_sum,
                                                    unsigned* __restrict__ status)
 {
+    // one link per thread; CTAs are dispatched in index order, so the CTAs in flight cover a
+    // contiguous window of the lattice and neighbours one t-slice away are still in L2
     double acc_thread = 0.0;
-    for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += gridDim.x * blockDim.x) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h < g.Vh) {
         const Site s = site_of(g, par, h);
         const Q<R> A = staple_update<R, MU>(U, g, s, par);
-        Q<R> out;
         if (KIND == SU2G_HEATBATH) {
-            double a = 0.0;
-            Q<R> old = U.ldh(MU, par, h);
-            out = heatbath_link<R>(A, old, beta, seed, (uint32_t)s.n, sweep, (uint32_t)MU, replica, a, status);
-            acc_thread += a;
+            Q<R> out;
+            if (heatbath_link<R>(A, beta, seed, (uint32_t)s.n, sweep, (uint32_t)MU, replica, acc_thread, out, status))
+                U.sth(MU, par, h, q_project(out));
         } else {
-            out = overrelax_link<R>(A, U.ldh(MU, par, h));
+            U.sth(MU, par, h, q_project(overrelax_link<R>(A, U.ldh(MU, par, h))));
         }
-        U.sth(MU, par, h, q_project(out));
     }
     if (KIND == SU2G_HEATBATH && acc_sum) {
         DD v = {acc_thread, 0.0};
@@ -173,7 +182,7 @@ void launch_update_t(su2g_lattice* h, int mu, int par, uint32_t sweep, double* a
 int launch_update(su2g_lattice* h, int kind, int mu, int par, uint32_t sweep, double* acc_sum)
 {
     const int cls = kind == SU2G_HEATBATH ? SU2G_K_HEATBATH : SU2G_K_OVERRELAX;
-    const int grid = grid_for(h, h->g.Vh, 8);
+    const int grid = (int)((h->g.Vh + kBlock - 1) / kBlock);
     launch_begin(h, cls);
     if (h->prec == SU2G_FP32) {
         if (kind == SU2G_HEATBATH) launch_update_t<float, SU2G_HEATBATH>(h, mu, par, sweep, acc_sum, grid);
