@@ -120,6 +120,20 @@ int su2g_qtop(su2g_lattice *h, double *q, double *sum_abs);
 int su2g_kp_histogram(su2g_lattice *h, double alpha, uint64_t seed, int64_t n, int32_t nbins,
                       int64_t *counts);
 
+/* ---- APE smearing without any allocation.  No counterpart in the reference.
+ * For callers that keep their field in device memory they obtained elsewhere and may not call
+ * cudaMalloc themselves (memory handed out by another component or a fixed budget, or loops that
+ * must not pay cudaMalloc's device-wide synchronisation), so they cannot create a handle.
+ * links: device pointer to the field in the reference's layout, double[V][4][4]; smeared in place,
+ * ns steps of `mode` with parameter alpha, enqueued on cuda_stream (NULL = default stream); the
+ * call does not synchronise.  The intermediate level lives in a static device array of 48 MiB
+ * that every GPU loading the library keeps until exit; lattices above 393216 sites are rejected
+ * with SU2G_EINVAL.  The first call on a device looks up that array's address (issue it before
+ * any stream capture).  All calls share the array: calls that overlap on the GPU race.  Errors
+ * are reported by su2g_last_error(NULL). */
+int su2g_ape_inplace_noalloc(double *links, const int32_t dims[4], int32_t ns, double alpha, int32_t mode,
+                             void *cuda_stream);
+
 /* ---- pinned (page-locked) host memory for field arrays, so that transfers run at full link
  * speed; the reference's pu block (init.c:842-858) can live in it. */
 int su2g_host_alloc(size_t bytes, void **ptr);

@@ -65,6 +65,7 @@ _SIGS = {
     "su2g_wilson": (ctypes.c_int, [_P, _I32P, _I32P, ctypes.c_int32, _DP]),
     "su2g_qtop": (ctypes.c_int, [_P, _DP, _DP]),
     "su2g_kp_histogram": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32, _I64P]),
+    "su2g_ape_inplace_noalloc": (ctypes.c_int, [_P, _I32P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _P]),
     "su2g_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_P)]),
     "su2g_host_free": (ctypes.c_int, [_P]),
     "su2g_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
