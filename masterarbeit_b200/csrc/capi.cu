@@ -44,6 +44,14 @@ int grid_for(const su2g_lattice* h, long long work, int per_sm)
     return (int)std::max<long long>(g, 1);
 }
 
+int resident_grid(const su2g_lattice* h, const void* kernel, long long work, size_t smem)
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return grid_for(h, work, per_sm);
+}
+
 static cudaEvent_t pool_event(su2g_lattice* h)
 {
     if (!h->event_pool.empty()) {

@@ -128,6 +128,10 @@ int check_cuda(su2g_lattice* h, cudaError_t e, const char* what);
 // on every SM, never more than needed, never more than kMaxPartials.
 int grid_for(const su2g_lattice* h, long long work, int per_sm);
 
+// Grid for a grid-stride kernel whose CTAs must all be resident at once (so that the CTAs in
+// flight sweep one contiguous window of the lattice): SMs x resident CTAs of `kernel` per SM.
+int resident_grid(const su2g_lattice* h, const void* kernel, long long work, size_t smem = 0);
+
 // Bracket a launch with profiling events when profiling is on; check the launch.
 int launch_begin(su2g_lattice* h, int cls);
 int launch_end(su2g_lattice* h, int cls, const char* what);

@@ -364,7 +364,8 @@ extern "C" int su2g_plaquette(su2g_lattice* h, double* p)
     if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_plaquette: null handle");
     if (!p) return set_error(h, SU2G_EINVAL, "su2g_plaquette: null output");
     cudaSetDevice(h->device);
-    const int grid = grid_for(h, h->g.V, 8);
+    const int grid = h->prec == SU2G_FP32 ? resident_grid(h, (const void*)k_plaquette<float>, h->g.V)
+                                          : resident_grid(h, (const void*)k_plaquette<double>, h->g.V);
     launch_begin(h, SU2G_K_PLAQUETTE);
     if (h->prec == SU2G_FP32)
         k_plaquette<float><<<grid, kBlock, 0, h->stream>>>(make_field<float>(h->dirp, h->g.Vh), h->g, h->partials);
@@ -422,7 +423,8 @@ extern "C" int su2g_wilson(su2g_lattice* h, const int32_t* R, const int32_t* T, 
     cudaSetDevice(h->device);
     int rc = ensure_partials(h, 8 * kWilsonTChunk);
     if (rc) return rc;
-    const int grid = grid_for(h, h->g.V, 4);
+    const int grid = h->prec == SU2G_FP32 ? resident_grid(h, (const void*)k_wilson<float, 8>, h->g.V)
+                                          : resident_grid(h, (const void*)k_wilson<double, 8>, h->g.V);
     std::vector<double> grid_w((size_t)rmax * tmax, 0.0);
     std::vector<char> want((size_t)rmax * tmax, 0);
     for (int i = 0; i < n; ++i) want[(size_t)(R[i] - 1) * tmax + (T[i] - 1)] = 1;
@@ -458,7 +460,8 @@ extern "C" int su2g_qtop(su2g_lattice* h, double* q, double* sum_abs)
     if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_qtop: null handle");
     if (!q) return set_error(h, SU2G_EINVAL, "su2g_qtop: null output");
     cudaSetDevice(h->device);
-    const int grid = grid_for(h, h->g.V, 4);
+    const int grid = h->prec == SU2G_FP32 ? resident_grid(h, (const void*)k_qtop<float>, h->g.V)
+                                          : resident_grid(h, (const void*)k_qtop<double>, h->g.V);
     launch_begin(h, SU2G_K_QTOP);
     if (h->prec == SU2G_FP32)
         k_qtop<float><<<grid, kBlock, 0, h->stream>>>(make_field<float>(h->dirp, h->g.Vh), h->g, h->partials);

@@ -27,8 +27,22 @@ __device__ __forceinline__ float eps_r<float>() { return FLT_EPSILON; }
 template <>
 __device__ __forceinline__ double eps_r<double>() { return DBL_EPSILON; }
 
-__device__ __forceinline__ float log_r(float x) { return logf(x); }
-__device__ __forceinline__ double log_r(double x) { return log(x); }
+// Sampler math.  FP64 uses the accurate library functions.  FP32 uses the hardware approximations
+// (__logf: absolute error ~2^-21 on (0,1]; __sincosf on [-pi, pi]: ~2^-21), which are below the
+// 2^-23 resolution of the FP32 uniforms' effect on delta and the angles.
+__device__ __forceinline__ float kp_log(float x) { return __logf(x); }
+__device__ __forceinline__ double kp_log(double x) { return log(x); }
+// cos and sin of 2 pi u for u in (0,1)
+__device__ __forceinline__ void kp_sincos2pi(float u, float* s, float* c)
+{
+    float ss, cc;
+    __sincosf(6.28318530717958647692f * (u - 0.5f), &ss, &cc);   // 2 pi (u - 1/2) in [-pi, pi]
+    *s = -ss;
+    *c = -cc;
+}
+__device__ __forceinline__ void kp_sincos2pi(double u, double* s, double* c) { sincospi(2.0 * u, s, c); }
+__device__ __forceinline__ float kp_cos2pi(float u) { return -__cosf(6.28318530717958647692f * (u - 0.5f)); }
+__device__ __forceinline__ double kp_cos2pi(double u) { return cospi(2.0 * u); }
 
 // Staple sum A with U_mu(x) A = sum of the six plaquettes containing U_mu(x)  (metro.c:34-63):
 //   A = sum_{nu != mu} U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag + U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu)
@@ -82,17 +96,18 @@ __device__ __forceinline__ Q<R> fallback_link(R r0, R r1, R r2)
 }
 
 // Kennedy-Pendleton heatbath of one link given its staple sum (heatbath.c:76-149).
-// Writes the new link to `out`; `acc` receives 1/trials (0 for the zero-staple fallback).  Returns
+// Writes the new link to `out` and the number of trials to `trials` (0 for the zero-staple
+// fallback; the reference counts 1/trials into its acceptance, heatbath.c:137, :148).  Returns
 // false only if the trial bound is hit (the link then keeps its old value).
 template <typename R>
 __device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t seed, uint32_t site, uint32_t sweep,
-                                              uint32_t mu, uint32_t replica, double& acc, Q<R>& out,
+                                              uint32_t mu, uint32_t replica, uint32_t& trials, Q<R>& out,
                                               unsigned* status)
 {
     const R k = sqrt_r(q_norm2(A));
     if (!(k > eps_r<R>())) {
         U4 w = link_random(seed, site, sweep, mu, 1u, 1u, kStreamUpdate, replica);
-        acc = 0.0;
+        trials = 0;
         out = fallback_link<R>(u01(w.x, R(0)), u01(w.y, R(0)), u01(w.z, R(0)));
         return true;
     }
@@ -104,24 +119,24 @@ __device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t se
         U4 w = link_random(seed, site, sweep, mu, trial, 0u, kStreamUpdate, replica);
         ++trial;
         const R u0 = u01(w.x, R(0)), u1 = u01(w.y, R(0)), u2 = u01(w.z, R(0)), u3 = u01(w.w, R(0));
-        const R c = cospi(R(2) * u2);
+        const R c = kp_cos2pi(u2);
         // X1 = -ln(u0)/alpha, X2 = -ln(u1)/alpha, delta = X2 + X1 cos^2(2 pi u2)  (heatbath.c:86-90)
-        delta = -(log_r(u1) + log_r(u0) * (c * c)) * ia;
+        delta = -(kp_log(u1) + kp_log(u0) * (c * c)) * ia;
         if (u3 * u3 <= R(1) - R(0.5) * delta) break;   // heatbath.c:94
         if (trial >= kMaxTrials) {   // the link keeps its value and the host sees the status bit
             atomicOr(status, kStatusKpTrials);
-            acc = 0.0;
+            trials = 0;
             return false;
         }
     }
-    acc = 1.0 / (double)trial;
+    trials = trial;
     // x0 = 1 - delta; (x1,x2,x3) = sqrt(1-x0^2) (sin th cos ph, sin th sin ph, cos th)  (heatbath.c:96-107)
     U4 w = link_random(seed, site, sweep, mu, 0u, 1u, kStreamUpdate, replica);
     const R a0 = u01(w.x, R(0)), a1 = u01(w.y, R(0));
     const R cth = R(1) - R(2) * a1;
     const R sth = R(2) * sqrt_r(a1 * (R(1) - a1));       // sin(acos(1 - 2 a1))
     R sph, cph;
-    sincospi(R(2) * a0, &sph, &cph);
+    kp_sincos2pi(a0, &sph, &cph);
     const R len = sqrt_r(delta * (R(2) - delta));          // sqrt(1 - (1-delta)^2)
     Q<R> X = q_make<R>(R(1) - delta, len * sth * cph, len * sth * sph, len * cth);
     // U = X V^dag, V = A/k  (heatbath.c:140-146)
@@ -153,8 +168,10 @@ __global__ void __launch_bounds__(kBlock) k_update(Field<R> U, Geom g, int par, 
         const Q<R> A = staple_update<R, MU>(U, g, s, par);
         if (KIND == SU2G_HEATBATH) {
             Q<R> out;
-            if (heatbath_link<R>(A, beta, seed, (uint32_t)s.n, sweep, (uint32_t)MU, replica, acc_thread, out, status))
+            uint32_t trials = 0;
+            if (heatbath_link<R>(A, beta, seed, (uint32_t)s.n, sweep, (uint32_t)MU, replica, trials, out, status))
                 U.sth(MU, par, h, q_project(out));
+            if (acc_sum && trials) acc_thread = 1.0 / (double)trials;
         } else {
             U.sth(MU, par, h, q_project(overrelax_link<R>(A, U.ldh(MU, par, h))));
         }

@@ -70,5 +70,21 @@ for spec in "${DIMS[@]}"; do
     gcc -mcmodel=large "$OUT/obj/ref_harness.o" "${objs[@]}" "$OUT/obj/ranlxd.o" -lm -o "$OUT/harness"
     gcc -mcmodel=large "$OUT/obj_inj/ref_harness.o" "${objs[@]}" "$OUT/obj_inj/inject_ranlxd.o" -lm \
         -o "$OUT/harness_inj"
+    # the reference's own, unmodified drivers (main/qcd.c, main_meas/meas.c, main_qtop/qtop.c)
+    extra=(modules/io/inp_IO.c modules/obs/2pt.c modules/dirac/dirac_wil.c modules/dirac/spin_alg.c
+           modules/dirac/sources.c modules/invert/solv_cg.c)
+    xobjs=()
+    for m in "${extra[@]}"; do
+        o="$OUT/obj/$(basename "${m%.c}").o"
+        gcc $CFLAGS -I"$OUT/include" -c "$LGT/$m" -o "$o" &
+        xobjs+=("$o")
+    done
+    for d in main/qcd.c main_meas/meas.c main_qtop/qtop.c; do
+        gcc $CFLAGS -I"$OUT/include" -c "$LGT/$d" -o "$OUT/obj/$(basename "${d%.c}").o" &
+    done
+    wait
+    for d in qcd meas qtop; do
+        gcc -mcmodel=large "$OUT/obj/$d.o" "${objs[@]}" "$OUT/obj/ranlxd.o" "${xobjs[@]}" -lm -o "$OUT/$d"
+    done
     echo "built $OUT"
 done
