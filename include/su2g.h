@@ -114,6 +114,18 @@ int su2g_wilson(su2g_lattice *h, const int32_t *R, const int32_t *T, int32_t n, 
  * receives sum_x |q(x)|, the scale against which the cancellation in Q is judged. */
 int su2g_qtop(su2g_lattice *h, double *q, double *sum_abs);
 
+/* ---- adjoint of the smeared charge (no counterpart in the reference, which has no derivative code):
+ * Q(U_N) after n_ape APE_all steps of parameter alpha (smearing_APE_all + topologicalCharge, the
+ * qtop.c:76-91 flow), and its vector-Jacobian product with respect to the handle's (unsmeared)
+ * field.  grad (may be NULL) receives, per link in the host order double[V][4][3], the su(2)
+ * coefficients g of dQ under U -> exp(eps X) U, X = i x.sigma:  dQ = eps * sum g.x + O(eps^2).
+ * The smeared levels are kept every `ckpt` steps (0 = ceil(sqrt(n_ape))) and recomputed in
+ * between.  The handle's field is not modified. */
+int su2g_ape_qtop_vjp(su2g_lattice *h, int32_t n_ape, double alpha, int32_t ckpt, double *q, double *grad);
+/* Levels the VJP keeps on the device and its device memory, for a given n_ape and ckpt. */
+int su2g_vjp_plan(const su2g_lattice *h, int32_t n_ape, int32_t ckpt, int32_t *levels_stored,
+                  int64_t *device_bytes);
+
 /* ---- Kennedy-Pendleton sampler alone (generateSU2InHeatbath_Improved, heatbath.c:76-121;
  * the reference's sampler test LGT_Code/main_test/test.c:115-166): counts of x0 in nbins
  * equal bins on [-1,1] for n draws at fixed alpha. */

@@ -148,4 +148,8 @@ int fetch_results(su2g_lattice* h, int off, int n);
 namespace su2g {
 // Enqueue `ns` smearing steps on the handle's stream (no synchronisation).
 int ape_enqueue(su2g_lattice* h, int ns, double alpha, int mode);
+// One smearing step from the field at in_dirs into out_dirs (only the smeared directions are written).
+int ape_step(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], int mode, double alpha);
+// Enqueue Q of the field at dirs; Q and sum|q| land in d_out[out_off], d_out[out_off + 1].
+int qtop_enqueue(su2g_lattice* h, void* const dirs[4], int out_off);
 }  // namespace su2g

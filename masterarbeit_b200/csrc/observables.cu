@@ -12,6 +12,7 @@
 #include <cmath>
 
 #include "internal.cuh"
+#include "clover.cuh"
 
 using namespace su2g;
 
@@ -229,65 +230,6 @@ __global__ void __launch_bounds__(kBlock) k_wilson(Field<R> U, Geom g, int r0, i
 
 // --------------------------------------------------- topological charge ---
 
-// Walk `steps` links along direction D (negative: backwards), multiplying the path product.
-// Forward: acc *= U_D(y), y += D.  Backward: y -= D, acc *= U_D(y)^dag  (computeLine,
-// topologicalcharge.c:18-44).
-template <typename R, int D>
-__device__ __forceinline__ void walk(const Field<R>& U, const Geom& g, int& n, int& c, int& par, int steps, Q<R>& acc)
-{
-    if (steps > 0) {
-        for (int i = 0; i < steps; ++i) {
-            acc = q_mul(acc, U.ld(D, par, n));
-            if (c == g.L[D] - 1) { n -= (g.L[D] - 1) * g.S[D]; c = 0; }
-            else { n += g.S[D]; ++c; }
-            par ^= 1;
-        }
-    } else {
-        for (int i = 0; i < -steps; ++i) {
-            if (c == 0) { n += (g.L[D] - 1) * g.S[D]; c = g.L[D] - 1; }
-            else { n -= g.S[D]; --c; }
-            par ^= 1;
-            acc = q_mul_nd(acc, U.ld(D, par, n));
-        }
-    }
-}
-
-// Improved clover field strength in plane (A, B) at site s:
-// F = [(k1 C1 + k2 C2 + k3 C3) - h.c.]/2 with C_e = (1/4) sum of the four e x e leaves and
-// (k1, k2, k3) = (1.5, -0.15, 1/90)  (computeCloverAverages / computeCloverProducts /
-// hermitianTraceless, topologicalcharge.c:46-162).  The leaves, all starting and ending at x:
-//   +A +B -A -B,   -B +A +B -A,   +B -A -B +A,   -A -B +A +B.
-template <typename R, int A, int B>
-__device__ __forceinline__ Q<R> clover_F(const Field<R>& U, const Geom& g, const Site& s, int par)
-{
-    const R kcoef[3] = {R(1.5), R(-0.15), R(1.0 / 90.0)};
-    Q<R> F = q_zero<R>();
-#pragma unroll
-    for (int e = 1; e <= 3; ++e) {
-        Q<R> C = q_zero<R>();
-        int n = s.n, ca = s.c[A], cb = s.c[B], p = par;
-        Q<R> l = q_one<R>();
-        walk<R, A>(U, g, n, ca, p, e, l); walk<R, B>(U, g, n, cb, p, e, l);
-        walk<R, A>(U, g, n, ca, p, -e, l); walk<R, B>(U, g, n, cb, p, -e, l);
-        C = q_add(C, l);
-        l = q_one<R>();
-        walk<R, B>(U, g, n, cb, p, -e, l); walk<R, A>(U, g, n, ca, p, e, l);
-        walk<R, B>(U, g, n, cb, p, e, l); walk<R, A>(U, g, n, ca, p, -e, l);
-        C = q_add(C, l);
-        l = q_one<R>();
-        walk<R, B>(U, g, n, cb, p, e, l); walk<R, A>(U, g, n, ca, p, -e, l);
-        walk<R, B>(U, g, n, cb, p, -e, l); walk<R, A>(U, g, n, ca, p, e, l);
-        C = q_add(C, l);
-        l = q_one<R>();
-        walk<R, A>(U, g, n, ca, p, -e, l); walk<R, B>(U, g, n, cb, p, -e, l);
-        walk<R, A>(U, g, n, ca, p, e, l); walk<R, B>(U, g, n, cb, p, e, l);
-        C = q_add(C, l);
-        F = q_axpy(kcoef[e - 1] * R(0.25), C, F);
-    }
-    F.c0 = R(0);   // (F - F^dag)/2 keeps the su(2) part
-    return F;
-}
-
 // q(x) = 8 [tr F01 F23 + tr F02 F31 + tr F03 F12], tr = 2 c0 (topologicalcharge.c:175-178)
 template <typename R>
 __device__ __forceinline__ double qtop_density(const Field<R>& U, const Geom& g, const Site& s, int par)
@@ -332,9 +274,9 @@ int ensure_alt(su2g_lattice* h)
 }
 
 template <typename R>
-void launch_ape(su2g_lattice* h, int mode, R alpha, int grid)
+void launch_ape(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], int mode, R alpha, int grid)
 {
-    Field<R> in = make_field<R>(h->dirp, h->g.Vh), out = make_field<R>(h->altp, h->g.Vh);
+    Field<R> in = make_field<R>(in_dirs, h->g.Vh), out = make_field<R>(out_dirs, h->g.Vh);
     if (mode == SU2G_APE_ALL) k_ape<R, SU2G_APE_ALL><<<grid, kBlock, 0, h->stream>>>(in, out, h->g, alpha);
     else if (mode == SU2G_APE_SPATIAL) k_ape<R, SU2G_APE_SPATIAL><<<grid, kBlock, 0, h->stream>>>(in, out, h->g, alpha);
     else k_ape<R, SU2G_APE_TEMPORAL><<<grid, kBlock, 0, h->stream>>>(in, out, h->g, alpha);
@@ -380,20 +322,40 @@ extern "C" int su2g_plaquette(su2g_lattice* h, double* p)
 }
 
 // Enqueue `ns` smearing steps without synchronising (used by su2g_ape and the adjoint).
+int su2g::ape_step(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], int mode, double alpha)
+{
+    const int grid = (int)((h->g.V + kBlock - 1) / kBlock);
+    launch_begin(h, SU2G_K_APE);
+    if (h->prec == SU2G_FP32) launch_ape<float>(h, in_dirs, out_dirs, mode, (float)alpha, grid);
+    else launch_ape<double>(h, in_dirs, out_dirs, mode, alpha, grid);
+    return launch_end(h, SU2G_K_APE, "APE kernel");
+}
+
 int su2g::ape_enqueue(su2g_lattice* h, int ns, double alpha, int mode)
 {
     int rc = ensure_alt(h);
     if (rc) return rc;
-    const int grid = (int)((h->g.V + kBlock - 1) / kBlock);
     for (int step = 0; step < ns; ++step) {
-        launch_begin(h, SU2G_K_APE);
-        if (h->prec == SU2G_FP32) launch_ape<float>(h, mode, (float)alpha, grid);
-        else launch_ape<double>(h, mode, alpha, grid);
-        if ((rc = launch_end(h, SU2G_K_APE, "APE kernel"))) return rc;
+        if ((rc = ape_step(h, h->dirp, h->altp, mode, alpha))) return rc;
         for (int mu = 0; mu < 4; ++mu)
             if (ape_updates(mode, mu)) std::swap(h->dirp[mu], h->altp[mu]);
     }
     return SU2G_OK;
+}
+
+int su2g::qtop_enqueue(su2g_lattice* h, void* const dirs[4], int out_off)
+{
+    const int grid = h->prec == SU2G_FP32 ? resident_grid(h, (const void*)k_qtop<float>, h->g.V)
+                                          : resident_grid(h, (const void*)k_qtop<double>, h->g.V);
+    launch_begin(h, SU2G_K_QTOP);
+    if (h->prec == SU2G_FP32)
+        k_qtop<float><<<grid, kBlock, 0, h->stream>>>(make_field<float>(dirs, h->g.Vh), h->g, h->partials);
+    else
+        k_qtop<double><<<grid, kBlock, 0, h->stream>>>(make_field<double>(dirs, h->g.Vh), h->g, h->partials);
+    int rc = launch_end(h, SU2G_K_QTOP, "topological charge kernel");
+    // Q = sum_x q(x) / (32 pi^2)  (topologicalcharge.c:194)
+    if (!rc) rc = finalize(h, grid, 2, 1.0 / (32.0 * kPi * kPi), out_off);
+    return rc;
 }
 
 extern "C" int su2g_ape(su2g_lattice* h, int32_t ns, double alpha, int32_t mode)
@@ -460,16 +422,7 @@ extern "C" int su2g_qtop(su2g_lattice* h, double* q, double* sum_abs)
     if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_qtop: null handle");
     if (!q) return set_error(h, SU2G_EINVAL, "su2g_qtop: null output");
     cudaSetDevice(h->device);
-    const int grid = h->prec == SU2G_FP32 ? resident_grid(h, (const void*)k_qtop<float>, h->g.V)
-                                          : resident_grid(h, (const void*)k_qtop<double>, h->g.V);
-    launch_begin(h, SU2G_K_QTOP);
-    if (h->prec == SU2G_FP32)
-        k_qtop<float><<<grid, kBlock, 0, h->stream>>>(make_field<float>(h->dirp, h->g.Vh), h->g, h->partials);
-    else
-        k_qtop<double><<<grid, kBlock, 0, h->stream>>>(make_field<double>(h->dirp, h->g.Vh), h->g, h->partials);
-    int rc = launch_end(h, SU2G_K_QTOP, "topological charge kernel");
-    // Q = sum_x q(x) / (32 pi^2)  (topologicalcharge.c:194)
-    if (!rc) rc = finalize(h, grid, 2, 1.0 / (32.0 * kPi * kPi), 0);
+    int rc = qtop_enqueue(h, h->dirp, 0);
     if (!rc) rc = fetch_results(h, 0, 2);
     if (!rc) {
         *q = h->h_out[0];

@@ -64,7 +64,9 @@ _SIGS = {
     "su2g_ape": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32]),
     "su2g_wilson": (ctypes.c_int, [_P, _I32P, _I32P, ctypes.c_int32, _DP]),
     "su2g_qtop": (ctypes.c_int, [_P, _DP, _DP]),
-    "su2g_kp_histogram": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32, _I64P]),
+    "su2g_ape_qtop_vjp": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _DP, _DP]),
+    "su2g_vjp_plan": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _I32P, _I64P]),
+    "su2g_kp_histogram":(ctypes.c_int, [_P, ctypes.c_double, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32, _I64P]),
     "su2g_ape_inplace_noalloc": (ctypes.c_int, [_P, _I32P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _P]),
     "su2g_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_P)]),
     "su2g_host_free": (ctypes.c_int, [_P]),
@@ -233,6 +235,19 @@ class Lattice:
         q, a = ctypes.c_double(), ctypes.c_double()
         self._check(self.lib.su2g_qtop(self.h, ctypes.byref(q), ctypes.byref(a)))
         return (q.value, a.value) if with_abs else q.value
+
+    def ape_qtop_vjp(self, n_ape, alpha, ckpt=0, grad=True):
+        """Q after n_ape APE_all steps and dQ/dU as su(2) coefficients per link, shape (V, 4, 3)."""
+        q = ctypes.c_double()
+        g = np.empty((self.volume, 4, 3), dtype=np.float64) if grad else None
+        self._check(self.lib.su2g_ape_qtop_vjp(self.h, int(n_ape), float(alpha), int(ckpt), ctypes.byref(q),
+                                               _as_dp(g) if grad else None))
+        return (q.value, g) if grad else q.value
+
+    def vjp_plan(self, n_ape, ckpt=0):
+        lev, nb = ctypes.c_int32(), ctypes.c_int64()
+        self._check(self.lib.su2g_vjp_plan(self.h, int(n_ape), int(ckpt), ctypes.byref(lev), ctypes.byref(nb)))
+        return lev.value, nb.value
 
     def kp_histogram(self, alpha, seed, n, nbins=200):
         c = np.zeros(nbins, dtype=np.int64)
