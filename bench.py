@@ -252,6 +252,51 @@ def time_steps(lat, K, fn):
     return lat.timer_end()
 
 
+def batch_figures(dist, sweeps=1000, seq_sweeps=20):
+    """Batched replicas: (a) 64 lattices 16 x 8^4, 16 x 10^4, 16 x 12^4, 16 x 16^4, beta ~ U[2.2, 3.2],
+    distinct seeds, alternating hot/cold, `sweeps` sweeps of 1 HB + 4 OR with the plaquette of every
+    replica every sweep, one CUDA-graph replay per sweep; (b) the same for 64 x 12^4 against 64 single
+    handles swept one after another (no graph)."""
+    import random
+    from masterarbeit_b200.su2g import Batch, Lattice
+
+    rng = random.Random(2024 + dist.rank)
+    out = {}
+
+    def specs(sizes):
+        return [{"dims": (L, L, L, L), "beta": rng.uniform(2.2, 3.2), "seed": 7000 + 97 * dist.rank + i,
+                 "replica": i, "start": "haar" if i % 2 else "cold"} for i, L in enumerate(sizes)]
+
+    for name, sizes in (("mixed_64", [8] * 16 + [10] * 16 + [12] * 16 + [16] * 16), ("uniform_64x12", [12] * 64)):
+        reps = specs(sizes)
+        upd = (1 + N_OR) * 4 * sum(L ** 4 for L in sizes)
+        B = Batch(reps, precision="fp32", device=dist.local)
+        block = B.autotune(1, N_OR)
+        B.run(10, 1, N_OR, 1)
+        trace, ms = B.run(sweeps, 1, N_OR, 1)
+        B.close()
+        ms_sweep_batch = ms / sweeps
+        Ls = [Lattice(r["dims"], precision="fp32", beta=r["beta"], seed=r["seed"], start=r["start"],
+                      replica=r["replica"], device=dist.local) for r in reps]
+        for L in Ls:
+            L.sweep(1, 1, N_OR)
+            L.plaquette()
+        t0 = time.perf_counter()
+        for _ in range(seq_sweeps):
+            for L in Ls:
+                L.sweep(1, 1, N_OR)
+                L.plaquette()
+        ms_sweep_seq = (time.perf_counter() - t0) * 1e3 / seq_sweeps
+        for L in Ls:
+            L.close()
+        out[name] = {"replicas": len(sizes), "sites": sum(L ** 4 for L in sizes), "autotuned_block": block,
+                     "sweeps": sweeps, "batched_ms_per_sweep": ms_sweep_batch,
+                     "batched_link_updates_per_s": upd / (ms_sweep_batch / 1e3),
+                     "sequential_ms_per_sweep": ms_sweep_seq, "speedup_vs_sequential": ms_sweep_seq / ms_sweep_batch,
+                     "plaquette_trace_finite": bool(trace is not None and all(map(math.isfinite, trace.ravel())))}
+    return out
+
+
 def run_ours(args, dist, dims):
     from masterarbeit_b200.su2g import Lattice, PinnedArray
 
@@ -353,6 +398,8 @@ def run_ours(args, dist, dims):
                 L.close()
         extras["fp32_over_fp64_link_updates"] = value / dist.world / extras["fp64_link_updates_per_s"]
         extras["fp32_over_fp64_ape_all"] = extras["fp32_ape_all_steps_per_s"] / extras["fp64_ape_all_steps_per_s"]
+    if not args.no_extras:
+        extras["batch"] = batch_figures(dist)
     line["extras"] = extras
 
     # end to end through the C ABI with host buffers: upload the configuration from pinned host

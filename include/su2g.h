@@ -126,6 +126,32 @@ int su2g_ape_qtop_vjp(su2g_lattice *h, int32_t n_ape, double alpha, int32_t ckpt
 int su2g_vjp_plan(const su2g_lattice *h, int32_t n_ape, int32_t ckpt, int32_t *levels_stored,
                   int64_t *device_bytes);
 
+/* ---- batched replicas: many independent lattices in one device pool, updated by one launch per
+ * checkerboard pass (no counterpart in the reference, whose thesis runs were one process per
+ * lattice).  Each replica draws the Philox streams of a single handle with the same seed and
+ * replica id, so results equal those of separate handles. */
+typedef struct su2g_batch su2g_batch;
+typedef struct su2g_replica {
+    int32_t dims[4];
+    double beta;
+    uint64_t seed;
+    uint32_t replica;    /* Philox stream id */
+    int32_t start;       /* su2g_start */
+} su2g_replica;
+int su2g_batch_create(const su2g_replica *reps, int32_t n, int32_t precision, int32_t device, su2g_batch **out);
+int su2g_batch_destroy(su2g_batch *b);
+const char *su2g_batch_last_error(const su2g_batch *b);
+/* n_sweeps sweeps of (n_hb heatbath + n_or overrelaxation); every meas_every sweeps the plaquette
+ * of every replica goes to plaq_trace[k * n + r] (k-th measurement; may be NULL; 0 = no
+ * measurement).  The block of meas_every sweeps plus measurement is one CUDA graph, replayed.
+ * ms (may be NULL) receives the device time of the replays. */
+int su2g_batch_run(su2g_batch *b, int32_t n_sweeps, int32_t n_hb, int32_t n_or, int32_t meas_every,
+                   double *plaq_trace, double *ms);
+/* Times the sweep for each candidate CTA size and keeps the fastest (the fields are restored). */
+int su2g_batch_autotune(su2g_batch *b, int32_t n_hb, int32_t n_or, int32_t *block_out);
+int su2g_batch_download(su2g_batch *b, int32_t r, double *links);
+int su2g_batch_upload(su2g_batch *b, int32_t r, const double *links);
+
 /* ---- Kennedy-Pendleton sampler alone (generateSU2InHeatbath_Improved, heatbath.c:76-121;
  * the reference's sampler test LGT_Code/main_test/test.c:115-166): counts of x0 in nbins
  * equal bins on [-1,1] for n draws at fixed alpha. */

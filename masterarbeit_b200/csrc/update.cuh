@@ -1,0 +1,146 @@
+// update.cuh -- per-link heatbath and overrelaxation (shared by the single-lattice and the
+// batched sweeps).  Reference: staples (LGT_Code/modules/update/metro.c:34-63),
+// generateSU2InHeatbath_Improved / localHeatbathUpdate (LGT_Code/modules/update/heatbath.c:76-149).
+#pragma once
+#include <cfloat>
+
+#include "internal.cuh"
+#include "philox.cuh"
+
+namespace su2g {
+
+template <typename R>
+__device__ __forceinline__ R eps_r();
+template <>
+__device__ __forceinline__ float eps_r<float>() { return FLT_EPSILON; }
+template <>
+__device__ __forceinline__ double eps_r<double>() { return DBL_EPSILON; }
+
+// Sampler math.  FP64 uses the accurate library functions.  FP32 uses the hardware approximations
+// (__logf: absolute error ~2^-21 on (0,1]; __sincosf on [-pi, pi]: ~2^-21), which are below the
+// 2^-23 resolution of the FP32 uniforms' effect on delta and the angles.
+__device__ __forceinline__ float kp_log(float x) { return __logf(x); }
+__device__ __forceinline__ double kp_log(double x) { return log(x); }
+// cos and sin of 2 pi u for u in (0,1)
+__device__ __forceinline__ void kp_sincos2pi(float u, float* s, float* c)
+{
+    float ss, cc;
+    __sincosf(6.28318530717958647692f * (u - 0.5f), &ss, &cc);   // 2 pi (u - 1/2) in [-pi, pi]
+    *s = -ss;
+    *c = -cc;
+}
+__device__ __forceinline__ void kp_sincos2pi(double u, double* s, double* c) { sincospi(2.0 * u, s, c); }
+__device__ __forceinline__ float kp_cos2pi(float u) { return -__cosf(6.28318530717958647692f * (u - 0.5f)); }
+__device__ __forceinline__ double kp_cos2pi(double u) { return cospi(2.0 * u); }
+
+// Staple sum A with U_mu(x) A = sum of the six plaquettes containing U_mu(x)  (metro.c:34-63):
+//   A = sum_{nu != mu} U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag + U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu)
+// All 18 links are loaded before the first product, so that a thread keeps every load of its
+// staple in flight at once (the pass is bound by memory latency x parallelism, not by ALU).
+template <typename R, int MU>
+__device__ __forceinline__ Q<R> staple_update(const Field<R>& U, const Geom& g, const Site& s, int par)
+{
+    const int q = par ^ 1;
+    const int dmu = up_off<MU>(g, s);
+    const int xmu = s.n + dmu;
+    Q<R> a[3], b[3], c[3], d[3], e[3], f[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int nu = k < MU ? k : k + 1;
+        const int xnu = s.n + up_off_rt(g, s.c, nu);
+        const int xmn = s.n + dn_off_rt(g, s.c, nu);
+        a[k] = U.ld(nu, q, xmu);           // U_nu(x+mu)
+        b[k] = U.ld(MU, q, xnu);           // U_mu(x+nu)
+        c[k] = U.ld(nu, par, s.n);         // U_nu(x)
+        d[k] = U.ld(nu, par, xmn + dmu);   // U_nu(x-nu+mu)
+        e[k] = U.ld(MU, q, xmn);           // U_mu(x-nu)
+        f[k] = U.ld(nu, q, xmn);           // U_nu(x-nu)
+    }
+    Q<R> A = q_zero<R>();
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        A = q_add(A, q_mul_nd(q_mul_nd(a[k], b[k]), c[k]));
+        A = q_add(A, q_mul_dn(q_mul(e[k], d[k]), f[k]));
+    }
+    return A;
+}
+
+// su2RandomMatrix (LGT_Code/modules/random/random_su3.c:141-155) for the zero-staple fallback.
+template <typename R>
+__device__ __forceinline__ Q<R> fallback_link(R r0, R r1, R r2)
+{
+    Q<R> u;
+    u.c0 = R(1) - R(2) * r0;
+    u.c1 = R(1) - R(2) * r1;
+    R zw = sqrt_r(R(1) - u.c1 * u.c1);
+    R s, c;
+    sincospi(R(2) * r2, &s, &c);
+    u.c2 = zw * c;
+    u.c3 = zw * s;
+    zw = sqrt_r(R(1) - u.c0 * u.c0);
+    u.c1 *= zw;
+    u.c2 *= zw;
+    u.c3 *= zw;
+    return u;
+}
+
+// Kennedy-Pendleton heatbath of one link given its staple sum (heatbath.c:76-149).
+// Writes the new link to `out` and the number of trials to `trials` (0 for the zero-staple
+// fallback; the reference counts 1/trials into its acceptance, heatbath.c:137, :148).  Returns
+// false only if the trial bound is hit (the link then keeps its old value).
+template <typename R>
+__device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t seed, uint32_t site, uint32_t sweep,
+                                              uint32_t mu, uint32_t replica, uint32_t& trials, Q<R>& out,
+                                              unsigned* status)
+{
+    const R k = sqrt_r(q_norm2(A));
+    if (!(k > eps_r<R>())) {
+        U4 w = link_random(seed, site, sweep, mu, 1u, 1u, kStreamUpdate, replica);
+        trials = 0;
+        out = fallback_link<R>(u01(w.x, R(0)), u01(w.y, R(0)), u01(w.z, R(0)));
+        return true;
+    }
+    const R ik = R(1) / k;
+    const R ia = R(1) / (k * beta);          // 1/alpha, alpha = k*beta (heatbath.c:142)
+    R delta;
+    uint32_t trial = 0;
+    for (;;) {
+        U4 w = link_random(seed, site, sweep, mu, trial, 0u, kStreamUpdate, replica);
+        ++trial;
+        const R u0 = u01(w.x, R(0)), u1 = u01(w.y, R(0)), u2 = u01(w.z, R(0)), u3 = u01(w.w, R(0));
+        const R c = kp_cos2pi(u2);
+        // X1 = -ln(u0)/alpha, X2 = -ln(u1)/alpha, delta = X2 + X1 cos^2(2 pi u2)  (heatbath.c:86-90)
+        delta = -(kp_log(u1) + kp_log(u0) * (c * c)) * ia;
+        if (u3 * u3 <= R(1) - R(0.5) * delta) break;   // heatbath.c:94
+        if (trial >= kMaxTrials) {   // the link keeps its value and the host sees the status bit
+            atomicOr(status, kStatusKpTrials);
+            trials = 0;
+            return false;
+        }
+    }
+    trials = trial;
+    // x0 = 1 - delta; (x1,x2,x3) = sqrt(1-x0^2) (sin th cos ph, sin th sin ph, cos th)  (heatbath.c:96-107)
+    U4 w = link_random(seed, site, sweep, mu, 0u, 1u, kStreamUpdate, replica);
+    const R a0 = u01(w.x, R(0)), a1 = u01(w.y, R(0));
+    const R cth = R(1) - R(2) * a1;
+    const R sth = R(2) * sqrt_r(a1 * (R(1) - a1));       // sin(acos(1 - 2 a1))
+    R sph, cph;
+    kp_sincos2pi(a0, &sph, &cph);
+    const R len = sqrt_r(delta * (R(2) - delta));          // sqrt(1 - (1-delta)^2)
+    Q<R> X = q_make<R>(R(1) - delta, len * sth * cph, len * sth * sph, len * cth);
+    // U = X V^dag, V = A/k  (heatbath.c:140-146)
+    out = q_mul_nd(X, q_scale(A, ik));
+    return true;
+}
+
+// Overrelaxation U' = (W U W)^dag with W = A/|A|: keeps Re tr(U A), and applied twice is the identity.
+template <typename R>
+__device__ __forceinline__ Q<R> overrelax_link(const Q<R>& A, const Q<R>& U)
+{
+    const R k2 = q_norm2(A);
+    if (!(k2 > eps_r<R>() * eps_r<R>())) return U;
+    const Q<R> W = q_scale(A, rsqrt_r(k2));
+    return q_dag(q_mul(q_mul(W, U), W));
+}
+
+}  // namespace su2g

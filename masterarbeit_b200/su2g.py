@@ -42,6 +42,16 @@ class Params(ctypes.Structure):
     ]
 
 
+class ReplicaSpec(ctypes.Structure):
+    _fields_ = [
+        ("dims", ctypes.c_int32 * 4),
+        ("beta", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+        ("replica", ctypes.c_uint32),
+        ("start", ctypes.c_int32),
+    ]
+
+
 _lib = None
 _P = ctypes.c_void_p
 _DP = ctypes.POINTER(ctypes.c_double)
@@ -68,6 +78,14 @@ _SIGS = {
     "su2g_vjp_plan": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _I32P, _I64P]),
     "su2g_kp_histogram":(ctypes.c_int, [_P, ctypes.c_double, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32, _I64P]),
     "su2g_ape_inplace_noalloc": (ctypes.c_int, [_P, _I32P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _P]),
+    "su2g_batch_create": (ctypes.c_int, [ctypes.POINTER(ReplicaSpec), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                         ctypes.POINTER(_P)]),
+    "su2g_batch_destroy": (ctypes.c_int, [_P]),
+    "su2g_batch_last_error": (ctypes.c_char_p, [_P]),
+    "su2g_batch_run": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]),
+    "su2g_batch_autotune": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _I32P]),
+    "su2g_batch_download": (ctypes.c_int, [_P, ctypes.c_int32, _DP]),
+    "su2g_batch_upload": (ctypes.c_int, [_P, ctypes.c_int32, _DP]),
     "su2g_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_P)]),
     "su2g_host_free": (ctypes.c_int, [_P]),
     "su2g_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
@@ -277,3 +295,68 @@ class Lattice:
             self._check(self.lib.su2g_profile_read(self.h, i, ctypes.byref(n), ctypes.byref(ms)))
             out[name] = (n.value, ms.value)
         return out
+
+
+class Batch:
+    """Many independent replicas (extents, beta, seed, start per replica) driven together."""
+
+    def __init__(self, replicas, precision="fp32", device=0):
+        """replicas: list of dicts with keys dims, beta, seed, replica (default: index), start."""
+        self.lib = load()
+        n = len(replicas)
+        arr = (ReplicaSpec * n)()
+        for i, r in enumerate(replicas):
+            for d in range(4):
+                arr[i].dims[d] = int(r["dims"][d])
+            arr[i].beta = float(r["beta"])
+            arr[i].seed = int(r["seed"])
+            arr[i].replica = int(r.get("replica", i))
+            s = r.get("start", "cold")
+            arr[i].start = START[s] if isinstance(s, str) else int(s)
+        prec = FP64 if str(precision).lower() in ("fp64", "f64", "double") else FP32
+        h = _P()
+        rc = self.lib.su2g_batch_create(arr, n, prec, int(device), ctypes.byref(h))
+        if rc != 0:
+            raise Su2gError(rc, self.lib.su2g_last_error(None).decode())
+        self.h = h
+        self.n = n
+        self.replicas = [dict(r) for r in replicas]
+
+    def _check(self, rc):
+        if rc != 0:
+            raise Su2gError(rc, self.lib.su2g_batch_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.su2g_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, n_sweeps, n_hb=1, n_or=0, meas_every=1):
+        """Returns (plaquette trace [n_sweeps // meas_every, n] or None, device ms)."""
+        nmeas = n_sweeps // meas_every if meas_every else 0
+        trace = np.empty((nmeas, self.n)) if nmeas else None
+        ms = ctypes.c_double()
+        self._check(self.lib.su2g_batch_run(self.h, int(n_sweeps), int(n_hb), int(n_or), int(meas_every),
+                                            _as_dp(trace) if trace is not None else None, ctypes.byref(ms)))
+        return trace, ms.value
+
+    def autotune(self, n_hb=1, n_or=4):
+        b = ctypes.c_int32()
+        self._check(self.lib.su2g_batch_autotune(self.h, int(n_hb), int(n_or), ctypes.byref(b)))
+        return b.value
+
+    def download(self, r):
+        V = int(np.prod(self.replicas[r]["dims"]))
+        a = np.empty((V, 4, 4))
+        self._check(self.lib.su2g_batch_download(self.h, int(r), _as_dp(a)))
+        return a
+
+    def upload(self, r, links):
+        a = np.ascontiguousarray(links, dtype=np.float64)
+        self._check(self.lib.su2g_batch_upload(self.h, int(r), _as_dp(a)))

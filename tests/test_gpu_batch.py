@@ -1,0 +1,92 @@
+"""Batched replicas: one launch per pass over many lattices of mixed extents, beta, seeds and starts,
+with the sweep + measurement block replayed from a CUDA graph."""
+import time
+
+import numpy as np
+import pytest
+
+from masterarbeit_b200 import Lattice
+from masterarbeit_b200.su2g import Batch
+
+pytestmark = pytest.mark.gpu
+
+REPS = [
+    {"dims": (4, 4, 4, 4), "beta": 2.5, "seed": 11, "replica": 0, "start": "cold"},
+    {"dims": (6, 4, 4, 8), "beta": 3.0, "seed": 12, "replica": 1, "start": "haar"},
+    {"dims": (8, 8, 8, 8), "beta": 2.2, "seed": 13, "replica": 2, "start": "ref"},
+    {"dims": (10, 10, 10, 10), "beta": 3.2, "seed": 14, "replica": 3, "start": "haar"},
+]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_equals_single_lattices(precision):
+    B = Batch(REPS, precision=precision)
+    trace, _ = B.run(3, n_hb=1, n_or=2, meas_every=1)
+    assert trace.shape == (3, len(REPS))
+    for i, r in enumerate(REPS):
+        L = Lattice(r["dims"], precision=precision, beta=r["beta"], seed=r["seed"], start=r["start"],
+                    replica=r["replica"])
+        for s in range(3):
+            L.sweep(1, 1, 2)
+            assert abs(trace[s, i] - L.plaquette()) <= 1e-14, (i, s)
+        assert np.array_equal(B.download(i), L.download()), i
+        L.close()
+    # a second run continues the same chains (Philox sweep index kept on the device)
+    trace2, _ = B.run(2, n_hb=1, n_or=2, meas_every=2)
+    L = Lattice(REPS[2]["dims"], precision=precision, beta=REPS[2]["beta"], seed=REPS[2]["seed"],
+                start=REPS[2]["start"], replica=2)
+    L.sweep(5, 1, 2)
+    assert abs(trace2[0, 2] - L.plaquette()) <= 1e-14
+    B.close()
+
+
+def test_autotune_leaves_the_chains_untouched():
+    B = Batch(REPS, precision="fp32")
+    B.run(2, 1, 1, 0)
+    before = [B.download(i) for i in range(len(REPS))]
+    block = B.autotune(1, 4)
+    assert block in (64, 128, 256)
+    for i in range(len(REPS)):
+        assert np.array_equal(B.download(i), before[i])
+    t1, _ = B.run(1, 1, 1, 1)
+    A = Batch(REPS, precision="fp32")
+    A.run(2, 1, 1, 0)
+    t2, _ = A.run(1, 1, 1, 1)
+    assert np.array_equal(t1, t2)
+
+
+def test_upload_download_roundtrip():
+    B = Batch(REPS[:2], precision="fp64")
+    U = B.download(1)
+    B.upload(0, B.download(0))
+    B.upload(1, U)
+    assert np.array_equal(B.download(1), U)
+
+
+def test_batched_beats_sequential_handles():
+    """64 replicas of 12^4 (beta in [2.2, 3.2], distinct seeds, alternating starts): one graph replay per
+    sweep for all replicas against 64 single handles swept one after another."""
+    rng = np.random.default_rng(5)
+    reps = [{"dims": (12, 12, 12, 12), "beta": float(rng.uniform(2.2, 3.2)), "seed": 1000 + i, "replica": i,
+             "start": "haar" if i % 2 else "cold"} for i in range(64)]
+    B = Batch(reps, precision="fp32")
+    B.autotune(1, 4)
+    B.run(5, 1, 4, 1)
+    nb = 50
+    _, ms_b = B.run(nb, 1, 4, 1)
+    Ls = [Lattice(r["dims"], precision="fp32", beta=r["beta"], seed=r["seed"], start=r["start"], replica=r["replica"])
+          for r in reps]
+    for L in Ls:
+        L.sweep(1, 1, 4)
+        L.plaquette()
+    ns = 5
+    t0 = time.perf_counter()
+    for _ in range(ns):
+        for L in Ls:
+            L.sweep(1, 1, 4)
+            L.plaquette()
+    t_seq = (time.perf_counter() - t0) / ns
+    t_bat = ms_b / 1e3 / nb
+    print(f"64 x 12^4: batched {t_bat * 1e3:.3f} ms/sweep, sequential {t_seq * 1e3:.3f} ms/sweep, "
+          f"speed-up {t_seq / t_bat:.1f}x")
+    assert t_seq / t_bat > 2.0
