@@ -122,6 +122,34 @@ int main(int argc, char *argv[])
         return 0;
     }
 
+    /* genw <start> <seed> <beta> <nsweeps> <every> <R,..> <T,..>: the qcd.c loop (heatbath sweep +
+     * plaquette per sweep) with measureWilsonLoop every `every` sweeps (the meas.c measurement) */
+    if (strcmp(cmd, "genw") == 0) {
+        if (argc != 9) die("genw <start> <seed> <beta> <nsweeps> <every> <R,..> <T,..>");
+        int start = atoi(argv[2]), seed = atoi(argv[3]), nsw = atoi(argv[5]), every = atoi(argv[6]);
+        static int R[256], T[256];
+        int nr = parse_list(argv[7], R, 256), nt = parse_list(argv[8], T, 256), tmax = 0;
+        if (nr != nt || every <= 0) die("bad W list or cadence");
+        for (int i = 0; i < nt; i++) tmax = T[i] > tmax ? T[i] : tmax;
+        measParams.mwil_mode = nr;
+        measParams.rExtents = R;
+        measParams.tExtents = T;
+        measParams.tf = tmax;
+        runParams.beta = atof(argv[4]);
+        rlxd_init(2, seed);
+        setup(start);
+        double w[256];
+        for (int n = 0; n < nsw; n++) {
+            gaugefieldUpdate(n + 1, 1, SIM_TYPE, SWEEP_TYPE);
+            printf("RESULT plaq %d %.17g\n", n + 1, plaquette());
+            if ((n + 1) % every == 0) {
+                measureWilsonLoop(w);
+                for (int i = 0; i < nr; i++) printf("RESULT wil %d %d %d %.17g\n", n + 1, R[i], T[i], w[i]);
+            }
+        }
+        return 0;
+    }
+
     /* plaq <cfg> */
     if (strcmp(cmd, "plaq") == 0) {
         if (argc != 3) die("plaq <cfg>");

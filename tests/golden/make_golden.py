@@ -107,6 +107,32 @@ def main():
             entry["hotinj"] = {"seed": 99, "plaq": float(rr[0][0]), "cfg": os.path.basename(out)}
         gold["lattices"][dims] = entry
 
+    # The reference's own heatbath chain (RANLUX) for the statistical comparison: qcd.c's loop at
+    # 8^4, beta = 3.09, cold start, plaquette every sweep, W(R,T) every 10 sweeps; the first
+    # THERM sweeps are discarded; errors by the t_int.c Gamma method (tests/_stats.py).
+    sys.path.insert(0, os.path.dirname(HERE))
+    import _stats
+    nsw, every, therm = 6000, 10, 500
+    R, T = [1, 2, 1, 2, 3], [1, 2, 2, 1, 3]
+    out = subprocess.run([harness("8x8x8x8"), "genw", "0", "1", "3.09", str(nsw), str(every), ",".join(map(str, R)),
+                          ",".join(map(str, T))], check=True, capture_output=True, text=True).stdout
+    plaq, wil = [], {}
+    for line in out.splitlines():
+        f = line.split()
+        if line.startswith("RESULT plaq"):
+            plaq.append((int(f[2]), float(f[3])))
+        elif line.startswith("RESULT wil"):
+            wil.setdefault((int(f[3]), int(f[4])), []).append((int(f[2]), float(f[5])))
+    chain = {"dims": [8, 8, 8, 8], "beta": 3.09, "start": "cold", "seed": 1, "sweeps": nsw, "therm": therm,
+             "sweep": "reference heatbath (lexicographic Gauss-Seidel), one sweep between plaquettes"}
+    m, e, t = _stats.mean_err([p for n, p in plaq if n > therm])
+    chain["plaquette"] = {"mean": m, "err": e, "tau_int": t}
+    chain["wilson"] = []
+    for (r_, t_), series in sorted(wil.items()):
+        m, e, t = _stats.mean_err([w for n, w in series if n > therm])
+        chain["wilson"].append({"R": r_, "T": t_, "every": every, "mean": m, "err": e, "tau_int": t})
+    gold["chain_8x8x8x8_b3.09"] = chain
+
     shutil.copyfile(os.path.join(REF, "LGT_Code", "main_test", "improved.dat"), os.path.join(HERE, "kp_improved.dat"))
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(gold, f, indent=1)
