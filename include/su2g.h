@@ -189,6 +189,12 @@ enum su2g_kernel_class {
     SU2G_K_WILSON = 4, SU2G_K_QTOP = 5, SU2G_K_REDUCE = 6, SU2G_K_OTHER = 7, SU2G_K_COUNT = 8
 };
 int su2g_profile_enable(su2g_lattice *h, int32_t enable);
+/* Kernel choice for a class (no reference counterpart).  SU2G_K_APE: 0 = the per-site kernel
+ * (default), 1 = the TMA-tiled FP32 APE_all kernel where the geometry allows it (plane tiles staged
+ * by cp.async.bulk; slower on B200 at 48^4 because its shared memory admits one CTA per SM). */
+int su2g_set_kernel_variant(su2g_lattice *h, int32_t kernel_class, int32_t variant);
+/* The variant an APE_all step of this handle runs (0 = per-site, 1 = TMA-tiled). */
+int su2g_kernel_variant(const su2g_lattice *h, int32_t kernel_class, int32_t *active);
 int su2g_profile_read(su2g_lattice *h, int32_t kernel_class, int64_t *launches, double *ms);
 
 #ifdef __cplusplus

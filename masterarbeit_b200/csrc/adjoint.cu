@@ -84,8 +84,9 @@ __global__ void __launch_bounds__(kBlock) k_qgrad_fbar(Field<R> U, Geom g, R* __
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.V) return;
-    const int par = i >= g.Vh, h = i - par * g.Vh;
-    const Site s = site_of(g, par, h);
+    int par;
+    const Site s = site_lex(g, i, par);
+    const int h = i >> 1;
     const size_t V = (size_t)g.V, n = (size_t)s.n;
     Q<R> f0 = clover_F<R, 0, 1>(U, g, s, par), f1 = clover_F<R, 2, 3>(U, g, s, par);
     stq(fbar, 0 * V + n, q_scale(f1, -scale));
@@ -182,8 +183,9 @@ __global__ void __launch_bounds__(kBlock) k_qgrad_scatter(Field<R> U, Field<R> G
     constexpr int A = plane_a(PLANE), B = plane_b(PLANE);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.V) return;
-    const int par = i >= g.Vh, h = i - par * g.Vh;
-    const Site s = site_of(g, par, h);
+    int par;
+    const Site s = site_lex(g, i, par);
+    const int h = i >> 1;
     const Q<R> Fbar = ldq(fbar, (size_t)PLANE * g.V + (size_t)s.n);
     clover_adjoint_e<R, A, B, 1>(U, G, g, s, par, Fbar);
     clover_adjoint_e<R, A, B, 2>(U, G, g, s, par, Fbar);
@@ -198,8 +200,9 @@ __global__ void __launch_bounds__(kBlock) k_ape_vbar(Field<R> U, Field<R> Gn, Fi
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.V) return;
-    const int par = i >= g.Vh, h = i - par * g.Vh, q = par ^ 1;
-    const Site s = site_of(g, par, h);
+    int par;
+    const Site s = site_lex(g, i, par);
+    const int h = i >> 1, q = par ^ 1;
     int xp[4], xm[4];
     Q<R> u[4];
 #pragma unroll
@@ -265,8 +268,9 @@ __global__ void __launch_bounds__(kBlock) k_ape_gather(Field<R> U, Field<R> Vb, 
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.V) return;
-    const int par = i >= g.Vh, h = i - par * g.Vh;
-    const Site s = site_of(g, par, h);
+    int par;
+    const Site s = site_lex(g, i, par);
+    const int h = i >> 1;
     switch (blockIdx.y) {
         case 0: gather_link<R, 0>(U, Vb, G, g, s, par, h, alpha); break;
         case 1: gather_link<R, 1>(U, Vb, G, g, s, par, h, alpha); break;
@@ -281,8 +285,9 @@ __global__ void __launch_bounds__(kBlock) k_grad_out(Field<R> G, Field<R> U, Geo
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.V) return;
-    const int par = i >= g.Vh, h = i - par * g.Vh;
-    const Site s = site_of(g, par, h);
+    int par;
+    const Site s = site_lex(g, i, par);
+    const int h = i >> 1;
 #pragma unroll
     for (int mu = 0; mu < 4; ++mu) {
         const Q<R> v = q_mul_nd(G.ldh(mu, par, h), U.ldh(mu, par, h));

@@ -84,7 +84,7 @@ __device__ __forceinline__ Field<R> rep_field(const Replica& r)
 }
 
 template <typename R, int MU, int KIND>
-__global__ void __launch_bounds__(256) k_batch_update(const Replica* __restrict__ reps, const int* __restrict__ map,
+__global__ void __launch_bounds__(256, 4) k_batch_update(const Replica* __restrict__ reps, const int* __restrict__ map,
                                                       const int* __restrict__ blk0, int par, int sub,
                                                       const uint32_t* __restrict__ ctr, unsigned* __restrict__ status)
 {
@@ -118,8 +118,9 @@ __global__ void __launch_bounds__(256) k_batch_plaquette(const Replica* __restri
     double site = 0.0;
     if (i < g.V) {
         const Field<R> U = rep_field<R>(rp);
-        const int par = i >= g.Vh, h = i - par * g.Vh, q = par ^ 1;
-        const Site s = site_of(g, par, h);
+        int par;
+        const Site s = site_lex(g, i, par);
+        const int h = i >> 1, q = par ^ 1;
 #pragma unroll
         for (int mu = 0; mu < 3; ++mu)
 #pragma unroll
@@ -170,8 +171,9 @@ __global__ void __launch_bounds__(256) k_batch_start(const Replica* __restrict__
     const int i = (blockIdx.x - blk0[r]) * blockDim.x + threadIdx.x;
     if (i >= g.V) return;
     const Field<R> U = rep_field<R>(rp);
-    const int par = i >= g.Vh, h = i - par * g.Vh;
-    const Site s = site_of(g, par, h);
+    int par;
+    const Site s = site_lex(g, i, par);
+    const int h = i >> 1;
     for (int mu = 0; mu < 4; ++mu) {
         Q<R> u = q_one<R>();
         if (rp.start != SU2G_START_COLD) {

@@ -112,6 +112,11 @@ int ensure_partials(su2g_lattice* h, size_t slots)
     return SU2G_OK;
 }
 
+int ensure_partial_entries(su2g_lattice* h, size_t n)
+{
+    return ensure_partials(h, (n + kMaxPartials - 1) / kMaxPartials);
+}
+
 __global__ void k_finalize(const DD* __restrict__ partials, int nparts, int stride, double scale,
                            double* __restrict__ out)
 {
@@ -122,11 +127,12 @@ __global__ void k_finalize(const DD* __restrict__ partials, int nparts, int stri
     if (threadIdx.x == 0) out[blockIdx.x] = (acc.s + acc.e) * scale;
 }
 
-int finalize(su2g_lattice* h, int nparts, int nslots, double scale, int out_off)
+int finalize(su2g_lattice* h, int nparts, int nslots, double scale, int out_off, int stride)
 {
     if (out_off + nslots > kOutSlots) return set_error(h, SU2G_EINVAL, "too many result slots");
     launch_begin(h, SU2G_K_REDUCE);
-    k_finalize<<<nslots, kBlock, 0, h->stream>>>(h->partials, nparts, kMaxPartials, scale, h->d_out + out_off);
+    k_finalize<<<nslots, kBlock, 0, h->stream>>>(h->partials, nparts, stride > 0 ? stride : kMaxPartials, scale,
+                                                  h->d_out + out_off);
     return launch_end(h, SU2G_K_REDUCE, "finalize reduction");
 }
 
@@ -144,6 +150,8 @@ int fetch_results(su2g_lattice* h, int off, int n)
     if (rc) return rc;
     if (status & kStatusKpTrials)
         return set_error(h, SU2G_EDEVICE, "a heatbath link exceeded %u Kennedy-Pendleton trials", kMaxTrials);
+    if (status & kStatusTmaTimeout)
+        return set_error(h, SU2G_EDEVICE, "a bulk copy into shared memory did not complete in time");
     if (status) return set_error(h, SU2G_EDEVICE, "device status word 0x%x", status);
     return SU2G_OK;
 }
@@ -307,6 +315,7 @@ extern "C" int su2g_create(const su2g_params* p, su2g_lattice** out)
     h->replica = p->replica;
     h->device = p->device;
     h->num_sms = prop.multiProcessorCount;
+    h->max_smem = (int)prop.sharedMemPerBlockOptin;
     h->link_bytes = p->precision == SU2G_FP32 ? 16 : 32;
 
     int rc = SU2G_OK;
@@ -525,4 +534,22 @@ extern "C" int su2g_host_free(void* ptr)
 {
     if (!ptr) return SU2G_OK;
     return check_cuda(nullptr, cudaFreeHost(ptr), "su2g_host_free");
+}
+
+extern "C" int su2g_set_kernel_variant(su2g_lattice* h, int32_t kernel_class, int32_t variant)
+{
+    if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_set_kernel_variant: null handle");
+    if (kernel_class != SU2G_K_APE || variant < 0 || variant > 1)
+        return set_error(h, SU2G_EINVAL, "su2g_set_kernel_variant: unknown class/variant (%d, %d)", kernel_class, variant);
+    h->ape_variant = variant;
+    return SU2G_OK;
+}
+
+extern "C" int su2g_kernel_variant(const su2g_lattice* h, int32_t kernel_class, int32_t* active)
+{
+    if (!h || !active) return set_error(nullptr, SU2G_EINVAL, "su2g_kernel_variant: null argument");
+    if (kernel_class != SU2G_K_APE) return set_error(nullptr, SU2G_EINVAL, "su2g_kernel_variant: unknown class");
+    const bool tma = h->prec == SU2G_FP32 && h->ape_variant == 1 && ape_tma_rows(h->g, h->max_smem) > 0;
+    *active = tma ? 1 : 0;
+    return SU2G_OK;
 }

@@ -17,7 +17,7 @@ constexpr int kOutSlots = 4096;        // device result doubles per handle
 constexpr uint32_t kMaxTrials = 1u << 20;   // Kennedy-Pendleton trials before a link gives up
 
 // Status bits a kernel may raise in the handle's status word.
-enum : unsigned { kStatusKpTrials = 1u, kStatusNonFinite = 2u };
+enum : unsigned { kStatusKpTrials = 1u, kStatusNonFinite = 2u, kStatusTmaTimeout = 4u };
 
 // Compensated sum: value s plus running error e (TwoSum, Knuth TAOCP vol. 2, 4.2.2).
 struct DD {
@@ -107,6 +107,8 @@ struct su2g_lattice {
     size_t aos_sites = 0;        // sites the staging buffer holds
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+    int max_smem = 0;            // opt-in shared memory per CTA
+    int ape_variant = 0;         // 0: per-site APE kernel, 1: TMA-tiled FP32 APE_all where it applies
     bool profiling = false;
     struct Prof {
         cudaEvent_t a, b;
@@ -136,10 +138,12 @@ int resident_grid(const su2g_lattice* h, const void* kernel, long long work, siz
 int launch_begin(su2g_lattice* h, int cls);
 int launch_end(su2g_lattice* h, int cls, const char* what);
 
-// Make sure the partial-sum scratch holds `slots` x kMaxPartials entries.
+// Make sure the partial-sum scratch holds `slots` x kMaxPartials entries (or at least n entries).
 int ensure_partials(su2g_lattice* h, size_t slots);
-// Launch k_finalize over `nslots` slots of `nparts` partials into d_out[out_off ...].
-int finalize(su2g_lattice* h, int nparts, int nslots, double scale, int out_off);
+int ensure_partial_entries(su2g_lattice* h, size_t n);
+// Launch k_finalize over `nslots` slots of `nparts` partials (slot k at partials[k * stride],
+// stride 0 = kMaxPartials) into d_out[out_off ...].
+int finalize(su2g_lattice* h, int nparts, int nslots, double scale, int out_off, int stride = 0);
 // Copy n result doubles from d_out[off] to h_out and synchronise; then check the status word.
 int fetch_results(su2g_lattice* h, int off, int n);
 
@@ -150,6 +154,9 @@ namespace su2g {
 int ape_enqueue(su2g_lattice* h, int ns, double alpha, int mode);
 // One smearing step from the field at in_dirs into out_dirs (only the smeared directions are written).
 int ape_step(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], int mode, double alpha);
+// TMA-tiled APE_all (FP32): rows per CTA if it applies to the geometry, else 0; and its launch.
+int ape_tma_rows(const Geom& g, int max_smem);
+int ape_tma_launch(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], double alpha, int yb);
 // Enqueue Q of the field at dirs; Q and sum|q| land in d_out[out_off], d_out[out_off + 1].
 int qtop_enqueue(su2g_lattice* h, void* const dirs[4], int out_off);
 }  // namespace su2g

@@ -70,6 +70,29 @@ __host__ __device__ __forceinline__ Q<R> q_mul_dn(const Q<R>& a, const Q<R>& b)
     return r;
 }
 
+// s + a*b and s + a*b^dag, written so that the accumulation folds into the multiply-adds
+template <typename R>
+__host__ __device__ __forceinline__ Q<R> q_mul_add(const Q<R>& s, const Q<R>& a, const Q<R>& b)
+{
+    Q<R> r;
+    r.c0 = s.c0 + a.c0 * b.c0 - a.c1 * b.c1 - a.c2 * b.c2 - a.c3 * b.c3;
+    r.c1 = s.c1 + a.c0 * b.c1 + a.c1 * b.c0 - a.c2 * b.c3 + a.c3 * b.c2;
+    r.c2 = s.c2 + a.c0 * b.c2 + a.c1 * b.c3 + a.c2 * b.c0 - a.c3 * b.c1;
+    r.c3 = s.c3 + a.c0 * b.c3 - a.c1 * b.c2 + a.c2 * b.c1 + a.c3 * b.c0;
+    return r;
+}
+
+template <typename R>
+__host__ __device__ __forceinline__ Q<R> q_mul_nd_add(const Q<R>& s, const Q<R>& a, const Q<R>& b)
+{
+    Q<R> r;
+    r.c0 = s.c0 + a.c0 * b.c0 + a.c1 * b.c1 + a.c2 * b.c2 + a.c3 * b.c3;
+    r.c1 = s.c1 - a.c0 * b.c1 + a.c1 * b.c0 + a.c2 * b.c3 - a.c3 * b.c2;
+    r.c2 = s.c2 - a.c0 * b.c2 - a.c1 * b.c3 + a.c2 * b.c0 + a.c3 * b.c1;
+    r.c3 = s.c3 - a.c0 * b.c3 + a.c1 * b.c2 - a.c2 * b.c1 + a.c3 * b.c0;
+    return r;
+}
+
 template <typename R>
 __host__ __device__ __forceinline__ Q<R> q_dag(const Q<R>& a) { return q_make<R>(a.c0, -a.c1, -a.c2, -a.c3); }
 
@@ -195,6 +218,37 @@ __device__ __forceinline__ Site site_of(const Geom& g, int parity, int h)
     s.c[0] = (int)t; s.c[1] = (int)x; s.c[2] = (int)y; s.c[3] = (int)(z + odd);
     s.n = (int)(n0 + odd);
     return s;
+}
+
+// Site with lexicographic index n; par receives its parity (t+x+y+z) & 1.  Kernels that visit every
+// site enumerate n in order, so that both parities of a region of the lattice are in flight
+// together (each link array is then streamed from DRAM once, not once per parity half).
+__device__ __forceinline__ Site site_lex(const Geom& g, int n, int& par)
+{
+    Site s;
+    uint32_t t = fdiv((uint32_t)n, g.dS0);
+    uint32_t r = (uint32_t)n - t * (uint32_t)g.S[0];
+    uint32_t x = fdiv(r, g.dS1);
+    r -= x * (uint32_t)g.S[1];
+    uint32_t y = fdiv(r, g.dS2);
+    uint32_t z = r - y * (uint32_t)g.S[2];
+    s.c[0] = (int)t; s.c[1] = (int)x; s.c[2] = (int)y; s.c[3] = (int)z;
+    s.n = n;
+    par = (int)((t + x + y + z) & 1u);
+    return s;
+}
+
+// Site visited by thread `tid` of CTA `cta` when CTAs alternate parity over the same run of h:
+// CTA 2k takes parity 0 and CTA 2k+1 parity 1 of h = k*ntid .. k*ntid+ntid-1.  A warp still reads
+// consecutive links of one array (full 128-bit coalescing), while the CTAs in flight cover both
+// parities of one region, so each array is streamed from DRAM once.  Grid: 2 * ceil(Vh / ntid).
+__device__ __forceinline__ bool site_cta_pair(const Geom& g, int cta, int tid, int ntid, Site& s, int& par, int& h)
+{
+    par = cta & 1;
+    h = (cta >> 1) * ntid + tid;
+    if (h >= g.Vh) return false;
+    s = site_of(g, par, h);
+    return true;
 }
 
 // Lexicographic index offset of the +mu / -mu neighbour of a site (periodic).

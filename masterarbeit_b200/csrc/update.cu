@@ -21,8 +21,11 @@ using namespace su2g;
 
 namespace {
 
+// At least 4 resident CTAs per SM (at most 64 registers a thread): measured at 48^4 on B200 against
+// 1, 2, 3 and 6, it is the fastest for both kinds and precisions (OR FP32 64 us, 92 % of the
+// measured copy bandwidth, against 79 us unbounded).
 template <typename R, int MU, int KIND>
-__global__ void __launch_bounds__(kBlock) k_update(Field<R> U, Geom g, int par, R beta, uint64_t seed, uint32_t sweep,
+__global__ void __launch_bounds__(kBlock, 4) k_update(Field<R> U, Geom g, int par, R beta, uint64_t seed, uint32_t sweep,
                                                    uint32_t replica, double* __restrict__ acc_sum,
                                                    unsigned* __restrict__ status)
 {

@@ -94,6 +94,8 @@ _SIGS = {
     "su2g_timer_end": (ctypes.c_int, [_P, _DP]),
     "su2g_profile_enable": (ctypes.c_int, [_P, ctypes.c_int32]),
     "su2g_profile_read": (ctypes.c_int, [_P, ctypes.c_int32, _I64P, _DP]),
+    "su2g_set_kernel_variant": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
+    "su2g_kernel_variant": (ctypes.c_int, [_P, ctypes.c_int32, _I32P]),
 }
 
 
@@ -283,6 +285,16 @@ class Lattice:
     def timer_end(self):
         v = ctypes.c_double()
         self._check(self.lib.su2g_timer_end(self.h, ctypes.byref(v)))
+        return v.value
+
+    def set_kernel_variant(self, kernel_class, variant):
+        cls = KERNEL_CLASSES.index(kernel_class) if isinstance(kernel_class, str) else int(kernel_class)
+        self._check(self.lib.su2g_set_kernel_variant(self.h, cls, int(variant)))
+
+    def kernel_variant(self, kernel_class):
+        cls = KERNEL_CLASSES.index(kernel_class) if isinstance(kernel_class, str) else int(kernel_class)
+        v = ctypes.c_int32()
+        self._check(self.lib.su2g_kernel_variant(self.h, cls, ctypes.byref(v)))
         return v.value
 
     def profile(self, enable=True):
