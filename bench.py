@@ -297,6 +297,35 @@ def batch_figures(dist, sweeps=1000, seq_sweeps=20):
     return out
 
 
+def graph_figures(dist, sweeps=200):
+    """The small-lattice chain of the reference's own test run (8^4, beta 3.09, cold start, seed 1,
+    `sweeps` x (1 HB + N_OR OR) with the plaquette after every sweep), issued call by call against
+    one replayed CUDA graph per sweep (su2g_graph_run)."""
+    from masterarbeit_b200.su2g import Lattice
+
+    out = {}
+    for prec in ("fp64", "fp32"):
+        a = Lattice((8, 8, 8, 8), precision=prec, beta=3.09, seed=1, start="cold", device=dist.local)
+        b = Lattice((8, 8, 8, 8), precision=prec, beta=3.09, seed=1, start="cold", device=dist.local)
+        a.sweep(5, 1, N_OR)
+        a.plaquette()
+        b.graph_run(5, 1, 1, N_OR)
+        t0 = time.perf_counter()
+        for _ in range(sweeps):
+            a.sweep(1, 1, N_OR)
+            a.plaquette()
+        plain = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        trace, _ = b.graph_run(sweeps, 1, 1, N_OR)
+        graph = time.perf_counter() - t0
+        out[f"{prec}_8x8x8x8"] = {"sweeps": sweeps, "plain_sweeps_per_s": sweeps / plain,
+                                  "graph_sweeps_per_s": sweeps / graph, "speedup": plain / graph,
+                                  "identical_to_plain": bool(abs(trace[-1] - a.plaquette()) == 0.0)}
+        a.close()
+        b.close()
+    return out
+
+
 def run_ours(args, dist, dims):
     from masterarbeit_b200.su2g import Lattice, PinnedArray
 
@@ -400,6 +429,7 @@ def run_ours(args, dist, dims):
         extras["fp32_over_fp64_ape_all"] = extras["fp32_ape_all_steps_per_s"] / extras["fp64_ape_all_steps_per_s"]
     if not args.no_extras:
         extras["batch"] = batch_figures(dist)
+        extras["graph_loop"] = graph_figures(dist)
     line["extras"] = extras
 
     # end to end through the C ABI with host buffers: upload the configuration from pinned host

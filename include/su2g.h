@@ -102,6 +102,17 @@ int su2g_sweep(su2g_lattice *h, int32_t n_sweeps, int32_t n_hb, int32_t n_or, do
  * overrelaxation.  For a heatbath pass, `sweep` is the Philox sweep index. */
 int su2g_update_pass(su2g_lattice *h, int32_t kind, int32_t mu, int32_t parity, uint32_t sweep);
 
+/* ---- the driver loop of LGT_Code/main/qcd.c:55-60 (gaugefieldUpdate, then plaquette) as one
+ * replayed CUDA graph.  Runs n_blocks blocks of [meas_every x (n_hb heatbath + n_or overrelaxation
+ * sweeps), plaquette].  The block is captured on first use and replayed; it is captured again
+ * when the block shape, beta, the seed or the field's buffers have changed.  The results equal
+ * those of the same su2g_sweep / su2g_plaquette sequence bit for bit.  plaq[b] and acc[b] (either
+ * may be NULL) receive the plaquette after block b and block b's mean heatbath acceptance. */
+int su2g_graph_run(su2g_lattice *h, int32_t n_blocks, int32_t meas_every, int32_t n_hb, int32_t n_or,
+                   double *plaq, double *acc);
+/* Free the captured block (it is also freed by su2g_destroy). */
+int su2g_graph_release(su2g_lattice *h);
+
 /* ---- observables */
 /* plaquette() (LGT_Code/modules/obs/plaquette.c:67-100): <(1/2) Re tr U_p> over 6V plaquettes. */
 int su2g_plaquette(su2g_lattice *h, double *p);

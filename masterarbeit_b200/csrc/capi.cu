@@ -359,6 +359,9 @@ extern "C" int su2g_destroy(su2g_lattice* h)
     for (auto e : h->event_pool) cudaEventDestroy(e);
     if (h->ev_begin) cudaEventDestroy(h->ev_begin);
     if (h->ev_end) cudaEventDestroy(h->ev_end);
+    release_run_graph(h);
+    cudaFree(h->d_run_ctr);
+    cudaFree(h->d_trace);
     cudaFree(h->field);
     cudaFree(h->field_alt);
     cudaFree(h->partials);

@@ -109,6 +109,19 @@ struct su2g_lattice {
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
     int max_smem = 0;            // opt-in shared memory per CTA
     int ape_variant = 0;         // 0: per-site APE kernel, 1: TMA-tiled FP32 APE_all where it applies
+    // Graph of one measurement block of su2g_run (recaptured when its key changes).
+    struct RunGraph {
+        cudaGraphExec_t exec = nullptr;
+        int meas_every = 0, n_hb = 0, n_or = 0;
+        double beta = 0.0;
+        uint64_t seed = 0;
+        const void* partials = nullptr;
+        const double* trace = nullptr;
+        void* dirp[4] = {nullptr, nullptr, nullptr, nullptr};
+    } run;
+    uint32_t* d_run_ctr = nullptr;   // [0] heatbath sweep index, [1] trace row (advanced by the graph)
+    double* d_trace = nullptr;       // per block: plaquette, acceptance
+    size_t trace_rows = 0;
     bool profiling = false;
     struct Prof {
         cudaEvent_t a, b;
@@ -159,4 +172,12 @@ int ape_tma_rows(const Geom& g, int max_smem);
 int ape_tma_launch(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], double alpha, int yb);
 // Enqueue Q of the field at dirs; Q and sum|q| land in d_out[out_off], d_out[out_off + 1].
 int qtop_enqueue(su2g_lattice* h, void* const dirs[4], int out_off);
+// Destroy the captured su2g_graph_run block, if any.
+void release_run_graph(su2g_lattice* h);
+// Enqueue the plaquette of the current field into d_out[out_off].
+int plaquette_enqueue(su2g_lattice* h, int out_off);
+// One (mu, parity) update pass.  The heatbath sweep index is `sweep`, plus *sweep_base when
+// sweep_base is given (a device counter, so that a captured graph advances it by itself).
+int launch_update(su2g_lattice* h, int kind, int mu, int par, uint32_t sweep, double* acc_sum,
+                  const uint32_t* sweep_base = nullptr);
 }  // namespace su2g

@@ -309,6 +309,14 @@ extern "C" int su2g_plaquette(su2g_lattice* h, double* p)
     if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_plaquette: null handle");
     if (!p) return set_error(h, SU2G_EINVAL, "su2g_plaquette: null output");
     cudaSetDevice(h->device);
+    int rc = plaquette_enqueue(h, 0);
+    if (!rc) rc = fetch_results(h, 0, 1);
+    if (!rc) *p = h->h_out[0];
+    return rc;
+}
+
+int su2g::plaquette_enqueue(su2g_lattice* h, int out_off)
+{
     const int grid = 2 * (int)((h->g.Vh + kBlock - 1) / kBlock);
     int rc = ensure_partial_entries(h, grid);
     if (rc) return rc;
@@ -319,9 +327,7 @@ extern "C" int su2g_plaquette(su2g_lattice* h, double* p)
         k_plaquette<double><<<grid, kBlock, 0, h->stream>>>(make_field<double>(h->dirp, h->g.Vh), h->g, h->partials);
     rc = launch_end(h, SU2G_K_PLAQUETTE, "plaquette kernel");
     // plaq = sum 2 c0 / (2 * 6 * V)  (plaquette.c:97); the kernel sums c0 = (1/2) Re tr
-    if (!rc) rc = finalize(h, grid, 1, 1.0 / (6.0 * (double)h->g.V), 0, grid);
-    if (!rc) rc = fetch_results(h, 0, 1);
-    if (!rc) *p = h->h_out[0];
+    if (!rc) rc = finalize(h, grid, 1, 1.0 / (6.0 * (double)h->g.V), out_off, grid);
     return rc;
 }
 

@@ -26,8 +26,8 @@ namespace {
 // measured copy bandwidth, against 79 us unbounded).
 template <typename R, int MU, int KIND>
 __global__ void __launch_bounds__(kBlock, 4) k_update(Field<R> U, Geom g, int par, R beta, uint64_t seed, uint32_t sweep,
-                                                   uint32_t replica, double* __restrict__ acc_sum,
-                                                   unsigned* __restrict__ status)
+                                                   const uint32_t* __restrict__ sweep_base, uint32_t replica,
+                                                   double* __restrict__ acc_sum, unsigned* __restrict__ status)
 {
     // one link per thread; CTAs are dispatched in index order, so the CTAs in flight cover a
     // contiguous window of the lattice and neighbours one t-slice away are still in L2
@@ -37,6 +37,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_update(Field<R> U, Geom g, int pa
         const Site s = site_of(g, par, h);
         const Q<R> A = staple_update<R, MU>(U, g, s, par);
         if (KIND == SU2G_HEATBATH) {
+            if (sweep_base) sweep += *sweep_base;
             Q<R> out;
             uint32_t trials = 0;
             if (heatbath_link<R>(A, beta, seed, (uint32_t)s.n, sweep, (uint32_t)MU, replica, trials, out, status))
@@ -54,32 +55,37 @@ __global__ void __launch_bounds__(kBlock, 4) k_update(Field<R> U, Geom g, int pa
 }
 
 template <typename R, int KIND>
-void launch_update_t(su2g_lattice* h, int mu, int par, uint32_t sweep, double* acc_sum, int grid)
+void launch_update_t(su2g_lattice* h, int mu, int par, uint32_t sweep, const uint32_t* base, double* acc_sum, int grid)
 {
     Field<R> U = make_field<R>(h->dirp, h->g.Vh);
     const R beta = (R)h->beta;
     switch (mu) {
-        case 0: k_update<R, 0, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, h->replica, acc_sum, h->d_status); break;
-        case 1: k_update<R, 1, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, h->replica, acc_sum, h->d_status); break;
-        case 2: k_update<R, 2, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, h->replica, acc_sum, h->d_status); break;
-        default: k_update<R, 3, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, h->replica, acc_sum, h->d_status); break;
+        case 0: k_update<R, 0, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        case 1: k_update<R, 1, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        case 2: k_update<R, 2, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        default: k_update<R, 3, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
     }
 }
 
-int launch_update(su2g_lattice* h, int kind, int mu, int par, uint32_t sweep, double* acc_sum)
+}  // namespace
+
+int su2g::launch_update(su2g_lattice* h, int kind, int mu, int par, uint32_t sweep, double* acc_sum,
+                        const uint32_t* base)
 {
     const int cls = kind == SU2G_HEATBATH ? SU2G_K_HEATBATH : SU2G_K_OVERRELAX;
     const int grid = (int)((h->g.Vh + kBlock - 1) / kBlock);
     launch_begin(h, cls);
     if (h->prec == SU2G_FP32) {
-        if (kind == SU2G_HEATBATH) launch_update_t<float, SU2G_HEATBATH>(h, mu, par, sweep, acc_sum, grid);
-        else launch_update_t<float, SU2G_OVERRELAX>(h, mu, par, sweep, acc_sum, grid);
+        if (kind == SU2G_HEATBATH) launch_update_t<float, SU2G_HEATBATH>(h, mu, par, sweep, base, acc_sum, grid);
+        else launch_update_t<float, SU2G_OVERRELAX>(h, mu, par, sweep, base, acc_sum, grid);
     } else {
-        if (kind == SU2G_HEATBATH) launch_update_t<double, SU2G_HEATBATH>(h, mu, par, sweep, acc_sum, grid);
-        else launch_update_t<double, SU2G_OVERRELAX>(h, mu, par, sweep, acc_sum, grid);
+        if (kind == SU2G_HEATBATH) launch_update_t<double, SU2G_HEATBATH>(h, mu, par, sweep, base, acc_sum, grid);
+        else launch_update_t<double, SU2G_OVERRELAX>(h, mu, par, sweep, base, acc_sum, grid);
     }
     return launch_end(h, cls, kind == SU2G_HEATBATH ? "heatbath pass" : "overrelaxation pass");
 }
+
+namespace {
 
 // ----------------------------------------------------------- sampler test ---
 

@@ -70,6 +70,8 @@ _SIGS = {
     "su2g_download_aos_f64": (ctypes.c_int, [_P, _DP]),
     "su2g_sweep": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP]),
     "su2g_update_pass": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]),
+    "su2g_graph_run": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]),
+    "su2g_graph_release": (ctypes.c_int, [_P]),
     "su2g_plaquette": (ctypes.c_int, [_P, _DP]),
     "su2g_ape": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32]),
     "su2g_wilson": (ctypes.c_int, [_P, _I32P, _I32P, ctypes.c_int32, _DP]),
@@ -234,6 +236,18 @@ class Lattice:
 
     def update_pass(self, kind, mu, parity, sweep=0):
         self._check(self.lib.su2g_update_pass(self.h, int(kind), int(mu), int(parity), int(sweep)))
+
+    def graph_run(self, n_blocks, meas_every=1, n_hb=1, n_or=0):
+        """n_blocks x [meas_every x (n_hb HB + n_or OR sweeps), plaquette] from one replayed CUDA
+        graph; returns (plaquette trace, acceptance trace), one entry per block."""
+        plaq = np.zeros(int(n_blocks))
+        acc = np.zeros(int(n_blocks))
+        self._check(self.lib.su2g_graph_run(self.h, int(n_blocks), int(meas_every), int(n_hb), int(n_or),
+                                            plaq.ctypes.data_as(_DP), acc.ctypes.data_as(_DP)))
+        return plaq, acc
+
+    def graph_release(self):
+        self._check(self.lib.su2g_graph_release(self.h))
 
     # -- observables
     def plaquette(self):
