@@ -43,7 +43,8 @@ enum su2g_status {
     SU2G_ENOMEM = -2,   /* device or pinned host allocation failed */
     SU2G_ECUDA = -3,    /* CUDA runtime error */
     SU2G_EDEVICE = -4,  /* a kernel reported a failure through its status word */
-    SU2G_ENODEV = -5    /* no usable sm_100 device */
+    SU2G_ENODEV = -5,   /* no usable sm_100 device */
+    SU2G_EFILE = -6     /* a configuration file could not be opened, read or written, or failed a check */
 };
 
 enum su2g_precision { SU2G_FP32 = 0, SU2G_FP64 = 1 };
@@ -101,6 +102,25 @@ int su2g_sweep(su2g_lattice *h, int32_t n_sweeps, int32_t n_hb, int32_t n_or, do
 /* One checkerboard pass: links of direction mu and site parity `parity`, heatbath or
  * overrelaxation.  For a heatbath pass, `sweep` is the Philox sweep index. */
 int su2g_update_pass(su2g_lattice *h, int32_t kind, int32_t mu, int32_t parity, uint32_t sweep);
+
+/* ---- configuration files in the reference's binary format (writeConfig / readConfig,
+ * LGT_Code/modules/io/config_IO.c:40-117, :537-621): int32 {4, 2}, int32 {L_t, L_x, L_y, L_z},
+ * the double plaquette, then for every site in lexicographic order and every direction the four
+ * doubles of the link; little-endian.  The links stream between the file and the device field
+ * through pinned double buffers, file I/O overlapping the copies and the layout conversion.
+ * su2g_read_config checks the header (dimension 4, SU(2), the handle's extents) and then the
+ * plaquette against the file's, |P - P_file| <= sqrt(6 V) DBL_EPSILON as readConfig does (for an
+ * FP32 handle, whose links are rounded on the way in, the bound is 1e-5).  plaq_file and plaq
+ * (either may be NULL) receive the file's and the computed plaquette.  On SU2G_EFILE the
+ * field may hold part of the file. */
+int su2g_read_config(su2g_lattice *h, const char *path, double *plaq_file, double *plaq);
+/* Writes the field with its plaquette (returned in plaq if not NULL) in the header. */
+int su2g_write_config(su2g_lattice *h, const char *path, double *plaq);
+/* readConfigForThermalisation (config_IO.c:348-535): the file holds a lattice of half the
+ * handle's extents in every direction; the field becomes its 16 mirror images, with the links
+ * along a mirrored direction daggered.  Same checks as su2g_read_config (the plaquette of the
+ * mirrored lattice equals the file's). */
+int su2g_read_config_reflect(su2g_lattice *h, const char *path, double *plaq_file, double *plaq);
 
 /* ---- the driver loop of LGT_Code/main/qcd.c:55-60 (gaugefieldUpdate, then plaquette) as one
  * replayed CUDA graph.  Runs n_blocks blocks of [meas_every x (n_hb heatbath + n_or overrelaxation

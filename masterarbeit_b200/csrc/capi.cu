@@ -261,7 +261,9 @@ __global__ void __launch_bounds__(kBlock) k_aos_out(double2* __restrict__ aos, F
 
 constexpr size_t kAosChunkSites = 1u << 20;   // 128 MB of FP64 AoS staging
 
-int ensure_aos(su2g_lattice* h)
+}  // namespace
+
+int su2g::ensure_aos(su2g_lattice* h)
 {
     if (h->d_aos) return SU2G_OK;
     size_t sites = std::min<size_t>((size_t)h->g.V, kAosChunkSites);
@@ -271,7 +273,31 @@ int ensure_aos(su2g_lattice* h)
     return SU2G_OK;
 }
 
-}  // namespace
+int su2g::aos_to_field(su2g_lattice* h, const double* d_src, size_t n0, int count)
+{
+    const int grid = grid_for(h, count, 8);
+    launch_begin(h, SU2G_K_OTHER);
+    if (h->prec == SU2G_FP32)
+        k_aos_in<float><<<grid, kBlock, 0, h->stream>>>((const double2*)d_src, make_field<float>(h->dirp, h->g.Vh), h->g,
+                                                       (int)n0, count);
+    else
+        k_aos_in<double><<<grid, kBlock, 0, h->stream>>>((const double2*)d_src, make_field<double>(h->dirp, h->g.Vh),
+                                                        h->g, (int)n0, count);
+    return launch_end(h, SU2G_K_OTHER, "layout conversion");
+}
+
+int su2g::field_to_aos(su2g_lattice* h, double* d_dst, size_t n0, int count)
+{
+    const int grid = grid_for(h, count, 8);
+    launch_begin(h, SU2G_K_OTHER);
+    if (h->prec == SU2G_FP32)
+        k_aos_out<float><<<grid, kBlock, 0, h->stream>>>((double2*)d_dst, make_field<float>(h->dirp, h->g.Vh), h->g,
+                                                        (int)n0, count);
+    else
+        k_aos_out<double><<<grid, kBlock, 0, h->stream>>>((double2*)d_dst, make_field<double>(h->dirp, h->g.Vh), h->g,
+                                                         (int)n0, count);
+    return launch_end(h, SU2G_K_OTHER, "layout conversion");
+}
 
 // ------------------------------------------------------------------- C ABI ---
 
@@ -432,16 +458,7 @@ extern "C" int su2g_upload_aos_f64(su2g_lattice* h, const double* links)
         rc = check_cuda(h, cudaMemcpyAsync(h->d_aos, links + n0 * 16, (size_t)cnt * 16 * sizeof(double),
                                            cudaMemcpyHostToDevice, h->stream),
                         "uploading links");
-        if (rc) return rc;
-        int grid = grid_for(h, cnt, 8);
-        launch_begin(h, SU2G_K_OTHER);
-        if (h->prec == SU2G_FP32)
-            k_aos_in<float><<<grid, kBlock, 0, h->stream>>>((const double2*)h->d_aos,
-                                                           make_field<float>(h->dirp, h->g.Vh), h->g, (int)n0, cnt);
-        else
-            k_aos_in<double><<<grid, kBlock, 0, h->stream>>>((const double2*)h->d_aos,
-                                                            make_field<double>(h->dirp, h->g.Vh), h->g, (int)n0, cnt);
-        if ((rc = launch_end(h, SU2G_K_OTHER, "layout conversion"))) return rc;
+        if (rc || (rc = aos_to_field(h, h->d_aos, n0, cnt))) return rc;
     }
     return check_cuda(h, cudaStreamSynchronize(h->stream), "uploading links");
 }
@@ -455,15 +472,7 @@ extern "C" int su2g_download_aos_f64(su2g_lattice* h, double* links)
     if (rc) return rc;
     for (size_t n0 = 0; n0 < (size_t)h->g.V; n0 += h->aos_sites) {
         int cnt = (int)std::min(h->aos_sites, (size_t)h->g.V - n0);
-        int grid = grid_for(h, cnt, 8);
-        launch_begin(h, SU2G_K_OTHER);
-        if (h->prec == SU2G_FP32)
-            k_aos_out<float><<<grid, kBlock, 0, h->stream>>>((double2*)h->d_aos, make_field<float>(h->dirp, h->g.Vh),
-                                                            h->g, (int)n0, cnt);
-        else
-            k_aos_out<double><<<grid, kBlock, 0, h->stream>>>((double2*)h->d_aos,
-                                                             make_field<double>(h->dirp, h->g.Vh), h->g, (int)n0, cnt);
-        if ((rc = launch_end(h, SU2G_K_OTHER, "layout conversion"))) return rc;
+        if ((rc = field_to_aos(h, h->d_aos, n0, cnt))) return rc;
         rc = check_cuda(h, cudaMemcpyAsync(links + n0 * 16, h->d_aos, (size_t)cnt * 16 * sizeof(double),
                                            cudaMemcpyDeviceToHost, h->stream),
                         "downloading links");

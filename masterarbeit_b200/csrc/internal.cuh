@@ -172,6 +172,11 @@ int ape_tma_rows(const Geom& g, int max_smem);
 int ape_tma_launch(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], double alpha, int yb);
 // Enqueue Q of the field at dirs; Q and sum|q| land in d_out[out_off], d_out[out_off + 1].
 int qtop_enqueue(su2g_lattice* h, void* const dirs[4], int out_off);
+// FP64 AoS staging (the reference's pu layout) and the conversions of sites [n0, n0 + count)
+// between a device AoS buffer and the handle's field.
+int ensure_aos(su2g_lattice* h);
+int aos_to_field(su2g_lattice* h, const double* d_src, size_t n0, int count);
+int field_to_aos(su2g_lattice* h, double* d_dst, size_t n0, int count);
 // Destroy the captured su2g_graph_run block, if any.
 void release_run_graph(su2g_lattice* h);
 // Enqueue the plaquette of the current field into d_out[out_off].

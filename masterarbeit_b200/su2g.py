@@ -72,6 +72,9 @@ _SIGS = {
     "su2g_update_pass": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]),
     "su2g_graph_run": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]),
     "su2g_graph_release": (ctypes.c_int, [_P]),
+    "su2g_read_config": (ctypes.c_int, [_P, ctypes.c_char_p, _DP, _DP]),
+    "su2g_write_config": (ctypes.c_int, [_P, ctypes.c_char_p, _DP]),
+    "su2g_read_config_reflect": (ctypes.c_int, [_P, ctypes.c_char_p, _DP, _DP]),
     "su2g_plaquette": (ctypes.c_int, [_P, _DP]),
     "su2g_ape": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32]),
     "su2g_wilson": (ctypes.c_int, [_P, _I32P, _I32P, ctypes.c_int32, _DP]),
@@ -248,6 +251,26 @@ class Lattice:
 
     def graph_release(self):
         self._check(self.lib.su2g_graph_release(self.h))
+
+    # -- configuration files (the reference's binary format)
+    def read_config(self, path):
+        """Stream a configuration file into the field; returns (file plaquette, computed plaquette)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.su2g_read_config(self.h, os.fsencode(path), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def write_config(self, path):
+        """Write the field to a configuration file; returns the plaquette stored in its header."""
+        v = ctypes.c_double()
+        self._check(self.lib.su2g_write_config(self.h, os.fsencode(path), ctypes.byref(v)))
+        return v.value
+
+    def read_config_reflect(self, path):
+        """readConfigForThermalisation: fill the field from a file of half the extents by 16
+        mirror images; returns (file plaquette, computed plaquette)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.su2g_read_config_reflect(self.h, os.fsencode(path), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     # -- observables
     def plaquette(self):

@@ -279,6 +279,17 @@ int main(int argc, char *argv[])
         return 0;
     }
 
+    /* reflect <small.cfg> <out.cfg>: readConfigForThermalisation (config_IO.c:348-535) of a
+     * configuration with half this build's extents, then writeConfig of the full lattice */
+    if (strcmp(cmd, "reflect") == 0) {
+        if (argc != 4) die("reflect <small.cfg> <out>");
+        setup(0);
+        readConfigForThermalisation(argv[2]);
+        printf("RESULT plaq %.17g\n", plaquette());
+        writeConfig(argv[3]);
+        return 0;
+    }
+
 #ifdef SU2_INJECT
     /* hotinj <seed> <out.cfg>: initGaugeField(1) on Philox uniforms (init.c:831-869) */
     if (strcmp(cmd, "hotinj") == 0) {

@@ -527,3 +527,46 @@ int su2o_kp_samples(double alpha, uint64_t seed, uint64_t n, double *x0)
     }
     return 0;
 }
+
+/* ------------------------------------------------------------- reflection --- */
+
+/* readConfigForThermalisation (LGT_Code/modules/io/config_IO.c:348-535): the field of extents
+ * dims is filled from one of extents dims/2 (`small`, same host layout) by 2^4 mirror images.
+ * Image k mirrors direction j when bit j of k is set (config_IO.c:448-456).  For small site c,
+ * link direction mu and image k the target coordinate along j is (config_IO.c:488-507)
+ *   L_j - c_j - 1                     mirrored, j == mu,
+ *   c_j == 0 ? L_j / 2 : L_j - c_j    mirrored, j != mu,
+ *   c_j                               not mirrored,
+ * and the stored link is U^dag when mu is mirrored (config_IO.c:510-517). */
+int su2o_reflect(const int dims[4], const double *small, double *U)
+{
+    lat_t g;
+    if (lat_init(&g, dims)) return -1;
+    int hl[4];
+    for (int j = 0; j < 4; ++j) {
+        if (dims[j] % 2) return -1;
+        hl[j] = dims[j] / 2;
+    }
+    const uint64_t vsmall = g.V / 16;
+    for (uint64_t in = 0; in < vsmall; ++in) {
+        int c[4];
+        uint64_t rem = in;
+        for (int j = 3; j >= 0; --j) {
+            c[j] = (int)(rem % (uint64_t)hl[j]);
+            rem /= (uint64_t)hl[j];
+        }
+        for (int mu = 0; mu < 4; ++mu) {
+            const qd u = ld(small, in, mu), ud = q_dag(u);
+            for (int k = 0; k < 16; ++k) {
+                uint64_t n = 0;
+                for (int j = 0; j < 4; ++j) {
+                    int x = c[j];
+                    if ((k >> j) & 1) x = (j == mu) ? dims[j] - c[j] - 1 : (c[j] == 0 ? hl[j] : dims[j] - c[j]);
+                    n = n * (uint64_t)dims[j] + (uint64_t)x;
+                }
+                st(U, n, mu, ((k >> mu) & 1) ? ud : u);
+            }
+        }
+    }
+    return 0;
+}

@@ -39,6 +39,7 @@ def lib():
                                  ctypes.c_uint32, _DP]
         L.su2o_link_action.argtypes = [_IP, _DP, _DP]
         L.su2o_kp_samples.argtypes = [ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64, _DP]
+        L.su2o_reflect.argtypes = [_IP, _DP, _DP]
         _lib = L
     return _lib
 
@@ -125,6 +126,14 @@ def kp_samples(alpha, seed, n):
     x = np.empty(int(n))
     _ok(lib().su2o_kp_samples(float(alpha), int(seed), int(n), _dp(x)))
     return x
+
+
+def reflect(dims, small):
+    """readConfigForThermalisation's 16 mirror images: a field of extents dims from one of dims/2."""
+    small = np.ascontiguousarray(small, dtype=np.float64)
+    out = np.zeros((int(np.prod(dims)), 4, 4))
+    _ok(lib().su2o_reflect(_dims(dims), _dp(small), _dp(out)))
+    return out
 
 
 def golden():

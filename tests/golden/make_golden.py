@@ -15,10 +15,16 @@ Outputs
   golden.json    observables computed by the reference's own routines
                  (%.17g): plaquette, APE, W(R,T), Q, injected-heatbath
                  acceptance and plaquette.
+  golden.json["reflect"]  readConfigForThermalisation of the 4x4x4x4 and 6x4x4x8 base
+                 configurations into lattices of twice the extents, run by the reference
+                 and written by its writeConfig: sha256 of the link payload (the bytes after
+                 the 32-byte header), the header plaquette and the computed one.  Run
+                 `make_golden.py --reflect-only` to refresh this part alone.
   kp_improved.dat  the reference's Kennedy-Pendleton sampler histogram at
                  alpha=7 (copied from LGT_Code/main_test/improved.dat; 200 bins
                  of N=1e8 draws; column 2 is count*200/N).
 """
+import hashlib
 import json
 import os
 import shutil
@@ -51,7 +57,32 @@ def run(cmd):
     return res
 
 
+REFLECT = {"4x4x4x4": "8x8x8x8", "6x4x4x8": "12x8x8x16"}   # small base -> full lattice
+
+
+def reflect_golden(gold):
+    subprocess.run([os.path.join(REPO, "oracle", "build_ref.sh"), REF] + sorted(set(REFLECT.values())), check=True)
+    out = {}
+    for small, big in REFLECT.items():
+        path = os.path.join("/tmp", f"reflect_{small}_to_{big}.cfg")
+        rr = run([harness(big), "reflect", os.path.join(HERE, f"cfg_{small}_base.cfg"), path])
+        with open(path, "rb") as f:
+            data = f.read()
+        out[big] = {"small": f"cfg_{small}_base.cfg", "plaq": float(rr[0][0]),
+                    "payload_sha256": hashlib.sha256(data[32:]).hexdigest(), "bytes": len(data)}
+    gold["reflect"] = out
+
+
 def main():
+    if "--reflect-only" in sys.argv:
+        path = os.path.join(HERE, "golden.json")
+        with open(path) as f:
+            gold = json.load(f)
+        reflect_golden(gold)
+        with open(path, "w") as f:
+            json.dump(gold, f, indent=1)
+        print("updated", path)
+        return 0
     subprocess.run([os.path.join(REPO, "oracle", "build_ref.sh"), REF] + list(LATTICES), check=True)
     gold = {"reference": "daggerfall247/Masterarbeit LGT_Code, compiled by oracle/build_ref.sh", "lattices": {}}
     for dims, (start, seed, beta, nsw) in LATTICES.items():
@@ -133,6 +164,7 @@ def main():
         chain["wilson"].append({"R": r_, "T": t_, "every": every, "mean": m, "err": e, "tau_int": t})
     gold["chain_8x8x8x8_b3.09"] = chain
 
+    reflect_golden(gold)
     shutil.copyfile(os.path.join(REF, "LGT_Code", "main_test", "improved.dat"), os.path.join(HERE, "kp_improved.dat"))
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(gold, f, indent=1)

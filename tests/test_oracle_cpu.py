@@ -1,5 +1,7 @@
 """Pin the CPU oracle to the reference: every oracle routine against the golden fixtures that the
 reference's own C code produced (tests/golden/make_golden.py).  No GPU needed."""
+import os
+
 import numpy as np
 import pytest
 
@@ -132,3 +134,22 @@ def test_kp_sampler_matches_reference_histogram():
     assert chi2a < dof + 5 * np.sqrt(2 * dof), (chi2a, dof)
     chi2r = np.sum((counts[m] - n * pref[m]) ** 2 / (n * pref[m]))
     assert chi2r < dof + 5 * np.sqrt(2 * dof), (chi2r, dof)
+
+
+@pytest.mark.parametrize("big", ["8x8x8x8", "12x8x8x16"])
+def test_reflection_matches_reference(golden, big):
+    """readConfigForThermalisation (config_IO.c:348-535): the oracle's 16 mirror images of the
+    half-size base configuration equal the reference's written lattice byte for byte, and the
+    plaquette is the small lattice's."""
+    import hashlib
+
+    from masterarbeit_b200.configio import read_config
+
+    g = golden["reflect"][big]
+    dims = tuple(int(x) for x in big.split("x"))
+    sdims, plaq0, small = read_config(os.path.join(O.GOLDEN, g["small"]))
+    assert tuple(2 * d for d in sdims) == dims
+    U = O.reflect(dims, small)
+    assert hashlib.sha256(U.astype("<f8").tobytes()).hexdigest() == g["payload_sha256"]
+    p = O.plaquette(dims, U)
+    assert abs(p - g["plaq"]) <= 1e-14 and abs(p - plaq0) <= 1e-13
