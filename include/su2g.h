@@ -122,6 +122,31 @@ int su2g_write_config(su2g_lattice *h, const char *path, double *plaq);
  * mirrored lattice equals the file's). */
 int su2g_read_config_reflect(su2g_lattice *h, const char *path, double *plaq_file, double *plaq);
 
+/* ---- one configuration's measurement in the meas and qtop drivers
+ * (LGT_Code/main_meas/meas.c:93-126, LGT_Code/main_qtop/qtop.c:76-91) as one replayed CUDA graph.
+ * Both branches start from a device copy of the handle's field, which is left unchanged:
+ *  - charges: q[i] = Q after q_ape[i] APE_all steps of parameter alpha_q (cumulative counts,
+ *    ascending; meas.c records one charge after smear_tc steps, qtop.c one per step count);
+ *  - loops: w[i] = W(R[i], T[i]) after ns_t temporal steps (alpha_t) and then ns_s spatial steps
+ *    (alpha_s), the tSmear / rSmear order of meas.c:106-109.
+ * The graph is captured on the first call with a given spec and replayed by later calls with the
+ * same spec (a new field read into the handle needs no new capture). */
+typedef struct su2g_meas_spec {
+    int32_t n_q;            /* charges to record (0: none) */
+    const int32_t *q_ape;   /* APE_all step count before each charge */
+    double alpha_q;
+    int32_t n_w;            /* Wilson loops to record (0: none) */
+    const int32_t *R;       /* spatial extents (measParams.rExtents) */
+    const int32_t *T;       /* temporal extents (measParams.tExtents), each <= L_t - 1 */
+    int32_t ns_t;           /* temporal APE steps before the loops (measParams.ismt) */
+    double alpha_t;         /* measParams.smpart */
+    int32_t ns_s;           /* spatial APE steps before the loops (measParams.isms) */
+    double alpha_s;         /* measParams.smpars */
+} su2g_meas_spec;
+int su2g_measure(su2g_lattice *h, const su2g_meas_spec *spec, double *q, double *w);
+/* Free the measurement graph and its two field copies (also freed by su2g_destroy). */
+int su2g_measure_release(su2g_lattice *h);
+
 /* ---- the driver loop of LGT_Code/main/qcd.c:55-60 (gaugefieldUpdate, then plaquette) as one
  * replayed CUDA graph.  Runs n_blocks blocks of [meas_every x (n_hb heatbath + n_or overrelaxation
  * sweeps), plaquette].  The block is captured on first use and replayed; it is captured again

@@ -14,6 +14,8 @@ REPO = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libsu2g.so")
+DRIVER_SRC = os.path.join(PKG, "driver", "su2meas.cpp")
+DRIVER = os.path.join(LIBDIR, "su2meas")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
@@ -44,6 +46,7 @@ def _stale():
 def build(force=False, verbose=False, extra=()):
     """Compile every .cu under csrc/ into one shared library; returns its path."""
     if not force and not _stale():
+        build_driver()
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     tmp = LIB + ".tmp"
@@ -57,7 +60,23 @@ def build(force=False, verbose=False, extra=()):
     if verbose and res.stderr:
         print(res.stderr, file=sys.stderr)
     os.replace(tmp, LIB)
+    build_driver(force=True)
     return LIB
+
+
+def build_driver(force=False):
+    """The native measurement driver (host C++ over the C ABI), next to the library."""
+    if not force and os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(
+            os.path.getmtime(DRIVER_SRC), os.path.getmtime(LIB)):
+        return DRIVER
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(REPO, "include"), DRIVER_SRC, "-L", LIBDIR,
+           "-lsu2g", "-Wl,-rpath,$ORIGIN", "-o", DRIVER + ".tmp"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("building su2meas failed:\n" + res.stdout + res.stderr)
+    os.replace(DRIVER + ".tmp", DRIVER)
+    return DRIVER
 
 
 if __name__ == "__main__":

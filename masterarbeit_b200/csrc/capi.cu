@@ -386,6 +386,9 @@ extern "C" int su2g_destroy(su2g_lattice* h)
     if (h->ev_begin) cudaEventDestroy(h->ev_begin);
     if (h->ev_end) cudaEventDestroy(h->ev_end);
     release_run_graph(h);
+    release_meas_graph(h);
+    cudaFree(h->meas_work);
+    cudaFree(h->meas_alt);
     cudaFree(h->d_run_ctr);
     cudaFree(h->d_trace);
     cudaFree(h->field);

@@ -13,7 +13,7 @@ namespace su2g {
 
 constexpr int kBlock = 256;            // threads per CTA for the stencil kernels
 constexpr int kMaxPartials = 8192;     // per-CTA partial sums a reduction may write
-constexpr int kOutSlots = 4096;        // device result doubles per handle
+constexpr int kOutSlots = 16384;       // device result doubles per handle
 constexpr uint32_t kMaxTrials = 1u << 20;   // Kennedy-Pendleton trials before a link gives up
 
 // Status bits a kernel may raise in the handle's status word.
@@ -84,6 +84,8 @@ __global__ void k_finalize(const DD* __restrict__ partials, int nparts, int stri
 
 }  // namespace su2g
 
+struct su2g_meas_graph;   // measure.cu
+
 struct su2g_lattice {
     su2g::Geom g;
     int prec = SU2G_FP32;
@@ -119,6 +121,9 @@ struct su2g_lattice {
         const double* trace = nullptr;
         void* dirp[4] = {nullptr, nullptr, nullptr, nullptr};
     } run;
+    su2g_meas_graph* meas = nullptr;   // graph of one su2g_measure spec
+    void* meas_work = nullptr;         // measurement copy of the field and its ping-pong partner
+    void* meas_alt = nullptr;
     uint32_t* d_run_ctr = nullptr;   // [0] heatbath sweep index, [1] trace row (advanced by the graph)
     double* d_trace = nullptr;       // per block: plaquette, acceptance
     size_t trace_rows = 0;
@@ -177,8 +182,17 @@ int qtop_enqueue(su2g_lattice* h, void* const dirs[4], int out_off);
 int ensure_aos(su2g_lattice* h);
 int aos_to_field(su2g_lattice* h, const double* d_src, size_t n0, int count);
 int field_to_aos(su2g_lattice* h, double* d_dst, size_t n0, int count);
+// Destroy the captured su2g_measure graph, if any.
+void release_meas_graph(su2g_lattice* h);
 // Destroy the captured su2g_graph_run block, if any.
 void release_run_graph(su2g_lattice* h);
+// Enqueue W(R[i], T[i]) of the field at dirs.  Loops are measured in chunks of R and T; each
+// chunk's results land in consecutive d_out slots from out_off on, and slot[i] receives the d_out
+// index of pair i.  Fails (nothing enqueued) if the pairs need more than `max_slots` slots.
+int wilson_enqueue(su2g_lattice* h, void* const dirs[4], const int32_t* R, const int32_t* T, int n, int out_off,
+                   int max_slots, int* slot);
+// Check R, T >= 1 and T <= L_t - 1 (measureWilsonLoop, wilson.c:290-291).
+int wilson_check(su2g_lattice* h, const int32_t* R, const int32_t* T, int n, const char* who);
 // Enqueue the plaquette of the current field into d_out[out_off].
 int plaquette_enqueue(su2g_lattice* h, int out_off);
 // One (mu, parity) update pass.  The heatbath sweep index is `sweep`, plus *sweep_base when

@@ -286,19 +286,19 @@ void launch_ape(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4]
 }
 
 template <typename R, int RC>
-void launch_wilson_t(su2g_lattice* h, int r0, int tlo, int thi, int grid)
+void launch_wilson_t(su2g_lattice* h, void* const dirs[4], int r0, int tlo, int thi, int grid)
 {
-    k_wilson<R, RC><<<grid, kBlock, 0, h->stream>>>(make_field<R>(h->dirp, h->g.Vh), h->g, r0, tlo, thi, h->partials);
+    k_wilson<R, RC><<<grid, kBlock, 0, h->stream>>>(make_field<R>(dirs, h->g.Vh), h->g, r0, tlo, thi, h->partials);
 }
 
 template <typename R>
-void launch_wilson(su2g_lattice* h, int rc, int r0, int tlo, int thi, int grid)
+void launch_wilson(su2g_lattice* h, void* const dirs[4], int rc, int r0, int tlo, int thi, int grid)
 {
     switch (rc) {
-        case 1: launch_wilson_t<R, 1>(h, r0, tlo, thi, grid); break;
-        case 2: launch_wilson_t<R, 2>(h, r0, tlo, thi, grid); break;
-        case 4: launch_wilson_t<R, 4>(h, r0, tlo, thi, grid); break;
-        default: launch_wilson_t<R, 8>(h, r0, tlo, thi, grid); break;
+        case 1: launch_wilson_t<R, 1>(h, dirs, r0, tlo, thi, grid); break;
+        case 2: launch_wilson_t<R, 2>(h, dirs, r0, tlo, thi, grid); break;
+        case 4: launch_wilson_t<R, 4>(h, dirs, r0, tlo, thi, grid); break;
+        default: launch_wilson_t<R, 8>(h, dirs, r0, tlo, thi, grid); break;
     }
 }
 
@@ -382,53 +382,92 @@ extern "C" int su2g_ape(su2g_lattice* h, int32_t ns, double alpha, int32_t mode)
     return ape_enqueue(h, ns, alpha, mode);
 }
 
+int su2g::wilson_check(su2g_lattice* h, const int32_t* R, const int32_t* T, int n, const char* who)
+{
+    int tmax = 0;
+    for (int i = 0; i < n; ++i) {
+        if (R[i] < 1 || T[i] < 1) return set_error(h, SU2G_EINVAL, "%s: R and T must be >= 1", who);
+        tmax = std::max(tmax, (int)T[i]);
+    }
+    // measureWilsonLoop refuses T > L_t - 1 (wilson.c:290-291)
+    if (tmax > h->g.L[0] - 1)
+        return set_error(h, SU2G_EINVAL, "%s: lattice too small to measure loops (T=%d, L_t=%d)", who, tmax, h->g.L[0]);
+    return SU2G_OK;
+}
+
+int su2g::wilson_enqueue(su2g_lattice* h, void* const dirs[4], const int32_t* R, const int32_t* T, int n, int out_off,
+                         int max_slots, int* slot)
+{
+    int rmax = 0, tmax = 0;
+    for (int i = 0; i < n; ++i) {
+        rmax = std::max(rmax, (int)R[i]);
+        tmax = std::max(tmax, (int)T[i]);
+    }
+    std::vector<char> want((size_t)rmax * tmax, 0);
+    for (int i = 0; i < n; ++i) want[(size_t)(R[i] - 1) * tmax + (T[i] - 1)] = 1;
+    // R in chunks of 8/4/2/1, T in chunks of kWilsonTChunk; a chunk with no wanted pair is skipped
+    struct Chunk {
+        int rc_n, r0, tlo, thi, base;
+    };
+    std::vector<Chunk> plan;
+    std::vector<int> slot_rt((size_t)rmax * tmax, -1);
+    int used = 0;
+    for (int r0 = 1; r0 <= rmax;) {
+        const int left = rmax - r0 + 1, rc_n = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
+        for (int tlo = 1; tlo <= tmax; tlo += kWilsonTChunk) {
+            const int thi = std::min(tmax, tlo + kWilsonTChunk - 1);
+            bool any = false;
+            for (int r = r0; r < r0 + rc_n; ++r)
+                for (int t = tlo; t <= thi; ++t) any = any || want[(size_t)(r - 1) * tmax + (t - 1)];
+            if (!any) continue;
+            plan.push_back({rc_n, r0, tlo, thi, out_off + used});
+            for (int r = 0; r < rc_n; ++r)
+                for (int t = tlo; t <= thi; ++t)
+                    slot_rt[(size_t)(r0 + r - 1) * tmax + (t - 1)] = out_off + used + r * kWilsonTChunk + (t - tlo);
+            used += rc_n * kWilsonTChunk;
+        }
+        r0 += rc_n;
+    }
+    if (used > max_slots)
+        return set_error(h, SU2G_EINVAL, "Wilson loops: %d result slots needed, %d available", used, max_slots);
+    int rc = ensure_partials(h, 8 * kWilsonTChunk);
+    if (rc) return rc;
+    const int grid = h->prec == SU2G_FP32 ? resident_grid(h, (const void*)k_wilson<float, 8>, h->g.V)
+                                          : resident_grid(h, (const void*)k_wilson<double, 8>, h->g.V);
+    for (const Chunk& c : plan) {
+        launch_begin(h, SU2G_K_WILSON);
+        if (h->prec == SU2G_FP32) launch_wilson<float>(h, dirs, c.rc_n, c.r0, c.tlo, c.thi, grid);
+        else launch_wilson<double>(h, dirs, c.rc_n, c.r0, c.tlo, c.thi, grid);
+        if ((rc = launch_end(h, SU2G_K_WILSON, "Wilson loop kernel"))) return rc;
+        // W = sum_x,k c0 / (3 V)  (wilson.c:322: sum of Re tr / (3 V 2))
+        if ((rc = finalize(h, grid, c.rc_n * kWilsonTChunk, 1.0 / (3.0 * (double)h->g.V), c.base))) return rc;
+    }
+    for (int i = 0; i < n; ++i) slot[i] = slot_rt[(size_t)(R[i] - 1) * tmax + (T[i] - 1)];
+    return SU2G_OK;
+}
+
 extern "C" int su2g_wilson(su2g_lattice* h, const int32_t* R, const int32_t* T, int32_t n, double* w)
 {
     if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_wilson: null handle");
     if (n < 0 || (n > 0 && (!R || !T || !w))) return set_error(h, SU2G_EINVAL, "su2g_wilson: bad argument");
     if (n == 0) return SU2G_OK;
-    int rmax = 0, tmax = 0;
-    for (int i = 0; i < n; ++i) {
-        if (R[i] < 1 || T[i] < 1) return set_error(h, SU2G_EINVAL, "su2g_wilson: R and T must be >= 1");
-        rmax = std::max(rmax, (int)R[i]);
-        tmax = std::max(tmax, (int)T[i]);
-    }
-    // measureWilsonLoop refuses T > L_t - 1 (wilson.c:290-291)
-    if (tmax > h->g.L[0] - 1)
-        return set_error(h, SU2G_EINVAL, "su2g_wilson: lattice too small to measure loops (T=%d, L_t=%d)", tmax,
-                         h->g.L[0]);
-    cudaSetDevice(h->device);
-    int rc = ensure_partials(h, 8 * kWilsonTChunk);
+    int rc = wilson_check(h, R, T, n, "su2g_wilson");
     if (rc) return rc;
-    const int grid = h->prec == SU2G_FP32 ? resident_grid(h, (const void*)k_wilson<float, 8>, h->g.V)
-                                          : resident_grid(h, (const void*)k_wilson<double, 8>, h->g.V);
-    std::vector<double> grid_w((size_t)rmax * tmax, 0.0);
-    std::vector<char> want((size_t)rmax * tmax, 0);
-    for (int i = 0; i < n; ++i) want[(size_t)(R[i] - 1) * tmax + (T[i] - 1)] = 1;
-    // R in chunks of 8/4/2/1, T in chunks of kWilsonTChunk; a chunk with no wanted pair is skipped
-    for (int r0 = 1; r0 <= rmax;) {
-        int left = rmax - r0 + 1, rc_n = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
-        for (int tlo = 1; tlo <= tmax; tlo += kWilsonTChunk) {
-            int thi = std::min(tmax, tlo + kWilsonTChunk - 1);
-            bool any = false;
-            for (int r = r0; r < r0 + rc_n; ++r)
-                for (int t = tlo; t <= thi; ++t) any = any || want[(size_t)(r - 1) * tmax + (t - 1)];
-            if (!any) continue;
-            launch_begin(h, SU2G_K_WILSON);
-            if (h->prec == SU2G_FP32) launch_wilson<float>(h, rc_n, r0, tlo, thi, grid);
-            else launch_wilson<double>(h, rc_n, r0, tlo, thi, grid);
-            if ((rc = launch_end(h, SU2G_K_WILSON, "Wilson loop kernel"))) return rc;
-            const int nslots = rc_n * kWilsonTChunk;
-            // W = sum_x,k c0 / (3 V)  (wilson.c:322: sum of Re tr / (3 V 2))
-            if ((rc = finalize(h, grid, nslots, 1.0 / (3.0 * (double)h->g.V), 0))) return rc;
-            if ((rc = fetch_results(h, 0, nslots))) return rc;
-            for (int r = 0; r < rc_n; ++r)
-                for (int t = tlo; t <= thi; ++t)
-                    grid_w[(size_t)(r0 + r - 1) * tmax + (t - 1)] = h->h_out[r * kWilsonTChunk + (t - tlo)];
-        }
-        r0 += rc_n;
+    cudaSetDevice(h->device);
+    // pairs are measured in groups whose chunks fit the result slots
+    std::vector<int> slot(n);
+    for (int i0 = 0; i0 < n;) {
+        int i1 = n;
+        while ((rc = wilson_enqueue(h, h->dirp, R + i0, T + i0, i1 - i0, 0, kOutSlots - 2, slot.data() + i0)) ==
+                   SU2G_EINVAL &&
+               i1 - i0 > 1)
+            i1 = i0 + (i1 - i0) / 2;
+        if (rc) return rc;
+        const int nres = 1 + *std::max_element(slot.begin() + i0, slot.begin() + i1);
+        if ((rc = fetch_results(h, 0, nres))) return rc;
+        for (int i = i0; i < i1; ++i) w[i] = h->h_out[slot[i]];
+        i0 = i1;
     }
-    for (int i = 0; i < n; ++i) w[i] = grid_w[(size_t)(R[i] - 1) * tmax + (T[i] - 1)];
     return SU2G_OK;
 }
 

@@ -52,6 +52,21 @@ class ReplicaSpec(ctypes.Structure):
     ]
 
 
+class MeasSpec(ctypes.Structure):
+    _fields_ = [
+        ("n_q", ctypes.c_int32),
+        ("q_ape", ctypes.POINTER(ctypes.c_int32)),
+        ("alpha_q", ctypes.c_double),
+        ("n_w", ctypes.c_int32),
+        ("R", ctypes.POINTER(ctypes.c_int32)),
+        ("T", ctypes.POINTER(ctypes.c_int32)),
+        ("ns_t", ctypes.c_int32),
+        ("alpha_t", ctypes.c_double),
+        ("ns_s", ctypes.c_int32),
+        ("alpha_s", ctypes.c_double),
+    ]
+
+
 _lib = None
 _P = ctypes.c_void_p
 _DP = ctypes.POINTER(ctypes.c_double)
@@ -75,6 +90,8 @@ _SIGS = {
     "su2g_read_config": (ctypes.c_int, [_P, ctypes.c_char_p, _DP, _DP]),
     "su2g_write_config": (ctypes.c_int, [_P, ctypes.c_char_p, _DP]),
     "su2g_read_config_reflect": (ctypes.c_int, [_P, ctypes.c_char_p, _DP, _DP]),
+    "su2g_measure": (ctypes.c_int, [_P, ctypes.POINTER(MeasSpec), _DP, _DP]),
+    "su2g_measure_release": (ctypes.c_int, [_P]),
     "su2g_plaquette": (ctypes.c_int, [_P, _DP]),
     "su2g_ape": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32]),
     "su2g_wilson": (ctypes.c_int, [_P, _I32P, _I32P, ctypes.c_int32, _DP]),
@@ -271,6 +288,25 @@ class Lattice:
         a, b = ctypes.c_double(), ctypes.c_double()
         self._check(self.lib.su2g_read_config_reflect(self.h, os.fsencode(path), ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def measure(self, q_ape=(), alpha_q=0.0, R=(), T=(), ns_t=0, alpha_t=0.0, ns_s=0, alpha_s=0.0):
+        """One measurement of the meas / qtop drivers on a copy of the field (one CUDA graph):
+        Q after each cumulative APE_all step count in q_ape, and W(R[i], T[i]) after ns_t temporal
+        and ns_s spatial steps.  Returns (q array, w array); the field is left unchanged."""
+        qa = (ctypes.c_int32 * max(1, len(q_ape)))(*[int(x) for x in q_ape])
+        Ra = (ctypes.c_int32 * max(1, len(R)))(*[int(x) for x in R])
+        Ta = (ctypes.c_int32 * max(1, len(T)))(*[int(x) for x in T])
+        if len(R) != len(T):
+            raise ValueError("R and T differ in length")
+        spec = MeasSpec(len(q_ape), qa, float(alpha_q), len(R), Ra, Ta, int(ns_t), float(alpha_t), int(ns_s),
+                        float(alpha_s))
+        q = np.zeros(max(1, len(q_ape)))
+        w = np.zeros(max(1, len(R)))
+        self._check(self.lib.su2g_measure(self.h, ctypes.byref(spec), q.ctypes.data_as(_DP), w.ctypes.data_as(_DP)))
+        return q[:len(q_ape)], w[:len(R)]
+
+    def measure_release(self):
+        self._check(self.lib.su2g_measure_release(self.h))
 
     # -- observables
     def plaquette(self):

@@ -108,3 +108,22 @@ def test_checkerboard_enumeration_is_a_bijection():
         for p in (0, 1):
             h = n[par == p] >> 1
             assert np.array_equal(np.sort(h), np.arange(V // 2))
+
+
+def test_su2meas_argument_and_input_errors(tmp_path):
+    """The native measurement driver refuses bad command lines, missing input files and two-point
+    functions before it touches a GPU."""
+    import subprocess
+
+    driver = os.path.join(O.REPO, "masterarbeit_b200", "_lib", "su2meas")
+    if not os.path.exists(driver):
+        pytest.skip("su2meas not built")
+    assert subprocess.run([driver], capture_output=True).returncode == 2
+    assert subprocess.run([driver, "-i", "x", "--qtop", "y", "-d", "4x4x4x4"], capture_output=True).returncode == 2
+    r = subprocess.run([driver, "-i", str(tmp_path / "none.in"), "-d", "4x4x4x4"], capture_output=True, text=True)
+    assert r.returncode == 1 and "unable to open input file" in r.stderr
+    inp = tmp_path / "meas.in"
+    inp.write_text("outFileId 1\nodir .\nbeta 3.09\nsconf 1\nfconf 1\neconf 1\nmtopcharge 0\nsmear_tc 0 0.1\n"
+                   "mwil 0 6\ntSmear 0 0.5\nrSmear 0 0.5\nmcorrs 1\n")
+    r = subprocess.run([driver, "-i", str(inp), "-d", "4x4x4x4"], capture_output=True, text=True)
+    assert r.returncode == 1 and "two-point functions" in r.stderr
