@@ -58,7 +58,7 @@ enum su2g_start { SU2G_START_COLD = 0, SU2G_START_HAAR = 1, SU2G_START_REF = 2 }
 enum su2g_ape_mode { SU2G_APE_ALL = 0, SU2G_APE_SPATIAL = 1, SU2G_APE_TEMPORAL = 2 };
 
 /* Update kinds for su2g_update_pass. */
-enum su2g_update_kind { SU2G_HEATBATH = 0, SU2G_OVERRELAX = 1 };
+enum su2g_update_kind { SU2G_HEATBATH = 0, SU2G_OVERRELAX = 1, SU2G_METROPOLIS = 2 };
 
 typedef struct su2g_params {
     int32_t dims[4];     /* L_t, L_x, L_y, L_z (headers.h:22-25 LENGT, LENGS1-3) */
@@ -98,6 +98,19 @@ int su2g_download_aos_f64(su2g_lattice *h, double *links);
  * receives the mean of 1/trials over all heatbath link updates (the `acc=` log value,
  * update.c:169-173) and the call synchronises; otherwise the call only enqueues. */
 int su2g_sweep(su2g_lattice *h, int32_t n_sweeps, int32_t n_hb, int32_t n_or, double *acc_out);
+
+/* gaugefieldUpdate(iup, nup, utype, stype) with both of the reference's update algorithms and
+ * sweep orders (update.c:102-175).  utype 1 = heatbath, 0 = Metropolis: localMetropolisUpdate
+ * (metro.c:78-109) with the proposal exp(eps X) U of proposeNewLink / expx (metro.c:65-76,
+ * exp_fct.c:137-151), step size eps (runParams.eps) and `hits` hits per visit (the reference's
+ * m = 1).  stype 0 = every link once per sweep; stype 1 = random site selection: V sites drawn
+ * with replacement (update.c:126-136), i.e. each site visited a Binomial(V, 1/V) number of times,
+ * a visit updating the site's four links.  Sweeps run as checkerboard passes, as su2g_sweep; a
+ * site's visits follow one another in its links' passes.  If acc_out is not NULL it receives the
+ * mean acceptance per link visit (update.c:164-171) and the call synchronises.  utype 1 with
+ * stype 0 is su2g_sweep(h, nup, 1, 0, acc_out). */
+int su2g_gauge_update(su2g_lattice *h, int32_t nup, int32_t utype, int32_t stype, double eps, int32_t hits,
+                      double *acc_out);
 
 /* One checkerboard pass: links of direction mu and site parity `parity`, heatbath or
  * overrelaxation.  For a heatbath pass, `sweep` is the Philox sweep index. */
@@ -242,7 +255,8 @@ int su2g_timer_end(su2g_lattice *h, double *ms);
  * kernel class, the launch count and summed device time since the last reset. */
 enum su2g_kernel_class {
     SU2G_K_HEATBATH = 0, SU2G_K_OVERRELAX = 1, SU2G_K_PLAQUETTE = 2, SU2G_K_APE = 3,
-    SU2G_K_WILSON = 4, SU2G_K_QTOP = 5, SU2G_K_REDUCE = 6, SU2G_K_OTHER = 7, SU2G_K_COUNT = 8
+    SU2G_K_WILSON = 4, SU2G_K_QTOP = 5, SU2G_K_REDUCE = 6, SU2G_K_OTHER = 7, SU2G_K_METROPOLIS = 8,
+    SU2G_K_COUNT = 9
 };
 int su2g_profile_enable(su2g_lattice *h, int32_t enable);
 /* Kernel choice for a class (no reference counterpart).  SU2G_K_APE: 0 = the per-site kernel

@@ -39,7 +39,8 @@ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1)
     return c;
 }
 
-enum : uint32_t { kStreamUpdate = 0u, kStreamStart = 1u };
+// Stream kinds: heatbath/fallback draws, starts, Metropolis hits, random-order visit counts.
+enum : uint32_t { kStreamUpdate = 0u, kStreamStart = 1u, kStreamMetro = 2u, kStreamVisit = 3u };
 
 __device__ __forceinline__ U4 link_random(uint64_t seed, uint32_t site, uint32_t sweep, uint32_t dir,
                                           uint32_t draw, uint32_t tag, uint32_t kind, uint32_t replica)

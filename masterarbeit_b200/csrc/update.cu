@@ -12,6 +12,7 @@
 // the sweep, update.c:166).  Randoms come from Philox keyed by (seed, site, sweep, dir, draw,
 // replica), so the result does not depend on grid shape or on which thread takes which link.
 #include <cfloat>
+#include <cmath>
 
 #include "internal.cuh"
 #include "philox.cuh"
@@ -52,6 +53,84 @@ __global__ void __launch_bounds__(kBlock, 4) k_update(Field<R> U, Geom g, int pa
         v = dd_block_sum<kBlock>(v);
         if (threadIdx.x == 0) atomicAdd(acc_sum, v.s + v.e);
     }
+}
+
+// The reference's other update algorithm and sweep order (gaugefieldUpdate's utype 0 and
+// stype 1, update.c:121-163): one link per thread as above, with
+//  - KIND = Metropolis: `hits` Metropolis hits per visit (metropolis_link);
+//  - ORDER = 1: a Binomial(V, 1/V) number of visits per site and sweep (visit_count, the same
+//    count for the site's four links), heatbath or Metropolis once per visit.
+// The acceptance sum counts 1/trials per heatbath visit and accepted/hits per Metropolis visit.
+struct VisitArgs {
+    double beta, eps;
+    int hits;
+    double p0;   // (1 - 1/V)^V
+    uint64_t seed;
+    uint32_t sweep, replica;
+};
+
+// Two resident CTAs per SM: the visit loop and the Metropolis state spill at 64 registers.
+template <typename R, int MU, int KIND, int ORDER>
+__global__ void __launch_bounds__(kBlock, 2) k_visit(Field<R> U, Geom g, int par, VisitArgs a,
+                                                  double* __restrict__ acc_sum, unsigned* __restrict__ status)
+{
+    double acc_thread = 0.0;
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h < g.Vh) {
+        const Site s = site_of(g, par, h);
+        int visits = 1;
+        if (ORDER == 1)
+            visits = visit_count(link_random(a.seed, (uint32_t)s.n, a.sweep, 0u, 0u, 0u, kStreamVisit, a.replica).x,
+                                 a.p0, (double)g.V);
+        if (visits > 0) {
+            const Q<R> A = staple_update<R, MU>(U, g, s, par);
+            if (KIND == SU2G_HEATBATH) {
+                Q<R> cur, out;
+                bool changed = false;
+                for (int v = 0; v < visits; ++v) {
+                    uint32_t trials = 0;
+                    if (heatbath_link<R>(A, (R)a.beta, a.seed, (uint32_t)s.n, a.sweep, (uint32_t)MU, a.replica, trials,
+                                         out, status, (uint32_t)v << kVisitShift)) {
+                        cur = out;
+                        changed = true;
+                    }
+                    if (trials) acc_thread += 1.0 / (double)trials;
+                }
+                if (changed) U.sth(MU, par, h, q_project(cur));
+            } else {
+                uint32_t accepted = 0;
+                const Q<R> u = metropolis_link<R>(A, U.ldh(MU, par, h), (R)a.beta, (R)a.eps, visits * a.hits, a.seed,
+                                                  (uint32_t)s.n, a.sweep, (uint32_t)MU, a.replica, accepted);
+                U.sth(MU, par, h, q_project(u));
+                acc_thread = (double)accepted / (double)a.hits;
+            }
+        }
+    }
+    if (acc_sum) {
+        DD v = {acc_thread, 0.0};
+        v = dd_block_sum<kBlock>(v);
+        if (threadIdx.x == 0) atomicAdd(acc_sum, v.s + v.e);
+    }
+}
+
+template <typename R, int KIND, int ORDER>
+void launch_visit_t(su2g_lattice* h, int mu, int par, const VisitArgs& a, double* acc_sum, int grid)
+{
+    Field<R> U = make_field<R>(h->dirp, h->g.Vh);
+    switch (mu) {
+        case 0: k_visit<R, 0, KIND, ORDER><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, a, acc_sum, h->d_status); break;
+        case 1: k_visit<R, 1, KIND, ORDER><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, a, acc_sum, h->d_status); break;
+        case 2: k_visit<R, 2, KIND, ORDER><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, a, acc_sum, h->d_status); break;
+        default: k_visit<R, 3, KIND, ORDER><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, a, acc_sum, h->d_status); break;
+    }
+}
+
+template <typename R>
+void launch_visit_r(su2g_lattice* h, int kind, int order, int mu, int par, const VisitArgs& a, double* acc_sum, int grid)
+{
+    if (kind == SU2G_HEATBATH) launch_visit_t<R, SU2G_HEATBATH, 1>(h, mu, par, a, acc_sum, grid);   // order 1 only
+    else if (order) launch_visit_t<R, SU2G_METROPOLIS, 1>(h, mu, par, a, acc_sum, grid);
+    else launch_visit_t<R, SU2G_METROPOLIS, 0>(h, mu, par, a, acc_sum, grid);
 }
 
 template <typename R, int KIND>
@@ -166,6 +245,56 @@ extern "C" int su2g_sweep(su2g_lattice* h, int32_t n_sweeps, int32_t n_hb, int32
         if ((rc = fetch_results(h, slot, 1))) return rc;
         const double nupd = (double)n_sweeps * n_hb * 4.0 * (double)h->g.V;
         *acc_out = nupd > 0 ? h->h_out[slot] / nupd : 0.0;
+    }
+    return SU2G_OK;
+}
+
+extern "C" int su2g_gauge_update(su2g_lattice* h, int32_t nup, int32_t utype, int32_t stype, double eps, int32_t hits,
+                                 double* acc_out)
+{
+    if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_gauge_update: null handle");
+    // the reference's checks and messages (update.c:109-113)
+    if (utype != 0 && utype != 1)
+        return set_error(h, SU2G_EINVAL, "su2g_gauge_update: unknown update type %d (Metropolis 0 and heatbath 1)", utype);
+    if (stype != 0 && stype != 1)
+        return set_error(h, SU2G_EINVAL, "su2g_gauge_update: unknown sweep type %d (sequential 0 and random 1)", stype);
+    if (nup < 0) return set_error(h, SU2G_EINVAL, "su2g_gauge_update: negative sweep count");
+    if (utype == 0 && (hits < 1 || !std::isfinite(eps)))
+        return set_error(h, SU2G_EINVAL, "su2g_gauge_update: Metropolis needs hits >= 1 and a finite step size");
+    if (utype == 1 && stype == 0) return su2g_sweep(h, nup, 1, 0, acc_out);
+    cudaSetDevice(h->device);
+    double* acc_dev = nullptr;
+    int rc = SU2G_OK;
+    if (acc_out) {
+        acc_dev = h->d_out;
+        if ((rc = check_cuda(h, cudaMemsetAsync(acc_dev, 0, sizeof(double), h->stream), "clearing acceptance")))
+            return rc;
+    }
+    VisitArgs a;
+    a.beta = h->beta;
+    a.eps = eps;
+    a.hits = utype == 0 ? hits : 1;
+    a.p0 = std::exp((double)h->g.V * std::log1p(-1.0 / (double)h->g.V));
+    a.seed = h->seed;
+    a.replica = h->replica;
+    const int kind = utype == 0 ? SU2G_METROPOLIS : SU2G_HEATBATH;
+    const int cls = kind == SU2G_HEATBATH ? SU2G_K_HEATBATH : SU2G_K_METROPOLIS;
+    const int grid = (int)((h->g.Vh + kBlock - 1) / kBlock);
+    for (int s = 0; s < nup; ++s) {
+        a.sweep = h->hb_sweeps;
+        for (int mu = 0; mu < 4; ++mu)
+            for (int par = 0; par < 2; ++par) {
+                launch_begin(h, cls);
+                if (h->prec == SU2G_FP32) launch_visit_r<float>(h, kind, stype, mu, par, a, acc_dev, grid);
+                else launch_visit_r<double>(h, kind, stype, mu, par, a, acc_dev, grid);
+                if ((rc = launch_end(h, cls, "update pass"))) return rc;
+            }
+        h->hb_sweeps++;
+    }
+    if (acc_out) {
+        if ((rc = fetch_results(h, 0, 1))) return rc;
+        const double nvis = (double)nup * 4.0 * (double)h->g.V;
+        *acc_out = nvis > 0 ? h->h_out[0] / nvis : 0.0;
     }
     return SU2G_OK;
 }

@@ -88,14 +88,17 @@ __device__ __forceinline__ Q<R> fallback_link(R r0, R r1, R r2)
 // Writes the new link to `out` and the number of trials to `trials` (0 for the zero-staple
 // fallback; the reference counts 1/trials into its acceptance, heatbath.c:137, :148).  Returns
 // false only if the trial bound is hit (the link then keeps its old value).
+// `draw_base` (visit << kVisitShift) separates the draws of repeated visits in a random-order sweep.
+constexpr int kVisitShift = 21;   // above every trial index (kMaxTrials = 2^20)
+
 template <typename R>
 __device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t seed, uint32_t site, uint32_t sweep,
                                               uint32_t mu, uint32_t replica, uint32_t& trials, Q<R>& out,
-                                              unsigned* status)
+                                              unsigned* status, uint32_t draw_base = 0u)
 {
     const R k = sqrt_r(q_norm2(A));
     if (!(k > eps_r<R>())) {
-        U4 w = link_random(seed, site, sweep, mu, 1u, 1u, kStreamUpdate, replica);
+        U4 w = link_random(seed, site, sweep, mu, draw_base | 1u, 1u, kStreamUpdate, replica);
         trials = 0;
         out = fallback_link<R>(u01(w.x, R(0)), u01(w.y, R(0)), u01(w.z, R(0)));
         return true;
@@ -105,7 +108,7 @@ __device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t se
     R delta;
     uint32_t trial = 0;
     for (;;) {
-        U4 w = link_random(seed, site, sweep, mu, trial, 0u, kStreamUpdate, replica);
+        U4 w = link_random(seed, site, sweep, mu, draw_base | trial, 0u, kStreamUpdate, replica);
         ++trial;
         const R u0 = u01(w.x, R(0)), u1 = u01(w.y, R(0)), u2 = u01(w.z, R(0)), u3 = u01(w.w, R(0));
         const R c = kp_cos2pi(u2);
@@ -120,7 +123,7 @@ __device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t se
     }
     trials = trial;
     // x0 = 1 - delta; (x1,x2,x3) = sqrt(1-x0^2) (sin th cos ph, sin th sin ph, cos th)  (heatbath.c:96-107)
-    U4 w = link_random(seed, site, sweep, mu, 0u, 1u, kStreamUpdate, replica);
+    U4 w = link_random(seed, site, sweep, mu, draw_base, 1u, kStreamUpdate, replica);
     const R a0 = u01(w.x, R(0)), a1 = u01(w.y, R(0));
     const R cth = R(1) - R(2) * a1;
     const R sth = R(2) * sqrt_r(a1 * (R(1) - a1));       // sin(acos(1 - 2 a1))
@@ -131,6 +134,55 @@ __device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t se
     // U = X V^dag, V = A/k  (heatbath.c:140-146)
     out = q_mul_nd(X, q_scale(A, ik));
     return true;
+}
+
+__device__ __forceinline__ float metro_exp(float x) { return __expf(x); }
+__device__ __forceinline__ double metro_exp(double x) { return exp(x); }
+
+// Metropolis hits on one link (localMetropolisUpdate, metro.c:78-109).  Hit i draws one Philox
+// block: X = (1 - 2 r0, 1 - 2 r1, 1 - 2 r2) (proposeNewLink, metro.c:65-76), the proposal is
+// exp(eps X) U with the O(X^2)-exact SU(2) exponential of expx (exp_fct.c:137-151), and it is
+// accepted when r3 <= exp(beta (Re tr(U' A) - Re tr(U A)) / 2).  Returns the new link; `accepted`
+// counts accepted hits.
+template <typename R>
+__device__ __forceinline__ Q<R> metropolis_link(const Q<R>& A, Q<R> U, R beta, R eps, int hits, uint64_t seed,
+                                                uint32_t site, uint32_t sweep, uint32_t mu, uint32_t replica,
+                                                uint32_t& accepted)
+{
+    R s_old = R(2) * q_mul(U, A).c0;   // Re tr(U A)
+    for (int i = 0; i < hits; ++i) {
+        U4 w = link_random(seed, site, sweep, mu, (uint32_t)i, 0u, kStreamMetro, replica);
+        const R x1 = R(1) - R(2) * u01(w.x, R(0)), x2 = R(1) - R(2) * u01(w.y, R(0)), x3 = R(1) - R(2) * u01(w.z, R(0));
+        R z = eps * eps * (x1 * x1 + x2 * x2 + x3 * x3) / R(4);
+        const R e0 = R(1) - z;
+        z = R(1) / (R(1) + z);
+        const R ze = z * eps;
+        const Q<R> P = q_mul(q_make<R>(e0 * z, ze * x1, ze * x2, ze * x3), U);
+        const R s_new = R(2) * q_mul(P, A).c0;
+        if (u01(w.w, R(0)) <= metro_exp(beta * (s_new - s_old) / R(2))) {
+            U = P;
+            s_old = s_new;
+            ++accepted;
+        }
+    }
+    return U;
+}
+
+// Times a site is drawn when V sites are drawn with replacement, as in gaugefieldUpdate's random
+// sweep (update.c:126-136): Binomial(V, 1/V), by inverting its CDF on one 32-bit uniform
+// (p0 = (1 - 1/V)^V, p_{k+1} = p_k (V - k) / ((k + 1)(V - 1))).  Computed in FP64 in both precision
+// modes, so FP32 and FP64 chains make the same visit decisions.
+__device__ __forceinline__ int visit_count(uint32_t w, double p0, double V)
+{
+    const double u = ((double)w + 0.5) * (1.0 / 4294967296.0);
+    double p = p0, c = p0;
+    int k = 0;
+    while (u > c && k < 32) {
+        p *= (V - k) / ((k + 1) * (V - 1.0));
+        c += p;
+        ++k;
+    }
+    return k;
 }
 
 // Overrelaxation U' = (W U W)^dag with W = A/|A|: keeps Re tr(U A), and applied twice is the identity.

@@ -116,8 +116,10 @@ static void to_host(void)
     }
 }
 
-/* gaugefieldUpdate, modules/update/update.c:102-175: nup heatbath sweeps (+ SU2G_OR
- * overrelaxation sweeps each), reprojection on every store, the same log lines. */
+/* gaugefieldUpdate, modules/update/update.c:102-175: nup sweeps of the heatbath (utype 1) or of
+ * Metropolis with step runParams.eps (utype 0), every link once (stype 0) or random site
+ * selection (stype 1); heatbath sequential sweeps are followed by SU2G_OR overrelaxation sweeps
+ * each.  Reprojection on every store, the same log lines. */
 void gaugefieldUpdate(int iup, int nup, int utype, int stype)
 {
     double acc = 0.0, t1, t2;
@@ -126,13 +128,15 @@ void gaugefieldUpdate(int iup, int nup, int utype, int stype)
           "Metropolis (SIM_TYPE=0) and heatbath (SIM_TYPE=1) implemented!");
     error(stype != 0 && stype != 1, "update [update.c]", "Unknown sweep type! "
           "Only sequential (SWEEP_TYPE=0) and random (SWEEP_TYPE=1) sweeps implemented!");
-    error(utype != 1, "update [ref_shim.c]", "The GPU path implements heatbath updates (SIM_TYPE=1) only");
-    error(stype != 0, "update [ref_shim.c]", "The GPU path implements checkerboard sweeps (SWEEP_TYPE=0) only");
 
     to_device();
     check(su2g_set_beta(g_h, runParams.beta), g_h, "su2g_set_beta [ref_shim.c]");
     t1 = getTime();
-    check(su2g_sweep(g_h, nup, 1, g_nor, &acc), g_h, "su2g_sweep [ref_shim.c]");
+    if (utype == 1 && stype == 0)
+        check(su2g_sweep(g_h, nup, 1, g_nor, &acc), g_h, "su2g_sweep [ref_shim.c]");
+    else
+        check(su2g_gauge_update(g_h, nup, utype, stype, runParams.eps, 1, &acc), g_h,
+              "su2g_gauge_update [ref_shim.c]");
     t2 = getTime();
     g_state = DEVICE_NEWER;
 

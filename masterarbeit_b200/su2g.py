@@ -17,7 +17,7 @@ FP32, FP64 = 0, 1
 START = {"cold": 0, "haar": 1, "ref": 2}
 APE = {"all": 0, "spatial": 1, "temporal": 2}
 HEATBATH, OVERRELAX = 0, 1
-KERNEL_CLASSES = ["heatbath", "overrelax", "plaquette", "ape", "wilson", "qtop", "reduce", "other"]
+KERNEL_CLASSES = ["heatbath", "overrelax", "plaquette", "ape", "wilson", "qtop", "reduce", "other", "metropolis"]
 
 _HEADER = os.path.join(_build.REPO, "include", "su2g.h")
 
@@ -92,6 +92,8 @@ _SIGS = {
     "su2g_read_config_reflect": (ctypes.c_int, [_P, ctypes.c_char_p, _DP, _DP]),
     "su2g_measure": (ctypes.c_int, [_P, ctypes.POINTER(MeasSpec), _DP, _DP]),
     "su2g_measure_release": (ctypes.c_int, [_P]),
+    "su2g_gauge_update": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                         ctypes.c_int32, _DP]),
     "su2g_plaquette": (ctypes.c_int, [_P, _DP]),
     "su2g_ape": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32]),
     "su2g_wilson": (ctypes.c_int, [_P, _I32P, _I32P, ctypes.c_int32, _DP]),
@@ -253,6 +255,15 @@ class Lattice:
             return v.value
         self._check(self.lib.su2g_sweep(self.h, n_sweeps, n_hb, n_or, None))
         return None
+
+    def gauge_update(self, nup=1, utype=1, stype=0, eps=0.15, hits=1):
+        """gaugefieldUpdate(iup, nup, utype, stype): utype 1 heatbath / 0 Metropolis (step eps,
+        `hits` hits per visit); stype 0 every link once / 1 random site selection.  Returns the
+        mean acceptance per link visit."""
+        v = ctypes.c_double()
+        self._check(self.lib.su2g_gauge_update(self.h, int(nup), int(utype), int(stype), float(eps), int(hits),
+                                                ctypes.byref(v)))
+        return v.value
 
     def update_pass(self, kind, mu, parity, sweep=0):
         self._check(self.lib.su2g_update_pass(self.h, int(kind), int(mu), int(parity), int(sweep)))

@@ -14,6 +14,9 @@
  *   heatbath.c:84    ranlxd(ud, 4)      once per Kennedy-Pendleton trial
  *   heatbath.c:97    ranlxd(angles, 2)  once after acceptance
  *   random_su3.c:145 ranlxd(r, 3)       zero-staple fallback / hot start
+ * and, in Metropolis mode (inject_set_metro), per hit of localMetropolisUpdate:
+ *   metro.c:71       ranlxd(r, 3)       the proposal: words 0..2 of block (stream METRO, draw = hit)
+ *   metro.c:98       ranlxd(r, 1)       the acceptance uniform: word 3 of the same block
  * The reference consumes ud[0], ud[1] as log(1 - ud); the GPU consumes log(u)
  * with u in (0,1).  We therefore hand out 1 - u for those two slots; for
  * u = (w + 0.5) 2^-32 both 1 - u and 1 - (1 - u) are exact in double, so the
@@ -28,6 +31,8 @@ static uint64_t g_seed = 0;
 static uint32_t g_site = 0, g_sweep = 0, g_dir = 0, g_replica = 0;
 static uint32_t g_trial = 0;
 static int g_init_mode = 0;
+static int g_metro = 0;
+static uint32_t g_metro_word = 0;
 static uint64_t g_init_link = 0;
 
 void inject_set_seed(uint64_t seed) { g_seed = seed; }
@@ -49,6 +54,8 @@ void inject_begin_init(void)
 
 void inject_end_init(void) { g_init_mode = 0; }
 
+void inject_set_metro(int on) { g_metro = on; }
+
 void ranlxd(double r[], int n)
 {
     uint32_t w[4];
@@ -61,6 +68,20 @@ void ranlxd(double r[], int n)
         su2_philox_link(g_seed, site, 0, dir, 0, 0, SU2_STREAM_INIT, g_replica, w);
         for (int i = 0; i < 3; ++i) r[i] = philox_u01_f64(w[i]);
         g_init_link++;
+        return;
+    }
+    if (g_metro) {
+        if (n == 3) {
+            su2_philox_link(g_seed, g_site, g_sweep, g_dir, g_trial, 0, SU2_STREAM_METRO, g_replica, w);
+            for (int i = 0; i < 3; ++i) r[i] = philox_u01_f64(w[i]);
+            g_metro_word = w[3];
+        } else if (n == 1) {
+            r[0] = philox_u01_f64(g_metro_word);
+            g_trial++;
+        } else {
+            fprintf(stderr, "inject_ranlxd: unexpected draw of %d in Metropolis mode\n", n);
+            exit(3);
+        }
         return;
     }
     if (n == 4) {

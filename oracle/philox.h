@@ -65,6 +65,9 @@ static inline float philox_u01_f32(uint32_t w)
 
 #define SU2_STREAM_UPDATE 0u
 #define SU2_STREAM_INIT 1u
+#define SU2_STREAM_METRO 2u
+#define SU2_STREAM_VISIT 3u
+#define SU2_VISIT_SHIFT 21   /* draw index of visit v's heatbath draws: (v << SU2_VISIT_SHIFT) | trial */
 
 static inline void su2_philox_link(uint64_t seed, uint32_t site, uint32_t sweep, uint32_t dir,
                                    uint32_t draw, uint32_t tag, uint32_t kind, uint32_t replica,

@@ -41,6 +41,7 @@ extern void inject_set_seed(uint64_t seed);
 extern void inject_set_link(uint32_t site, uint32_t dir, uint32_t sweep);
 extern void inject_begin_init(void);
 extern void inject_end_init(void);
+extern void inject_set_metro(int on);
 #endif
 
 static void die(const char *msg)
@@ -119,6 +120,24 @@ int main(int argc, char *argv[])
             printf("RESULT plaq %d %.17g\n", n + 1, plaquette());
         }
         writeConfig(argv[6]);
+        return 0;
+    }
+
+    /* genm <start> <seed> <beta> <eps> <utype> <stype> <nsweeps>: the qcd.c loop with any of the
+     * reference's update algorithms (utype 0 Metropolis, 1 heatbath) and sweep orders (stype 0
+     * sequential, 1 random sites), update.c:102-175, plaquette after every sweep */
+    if (strcmp(cmd, "genm") == 0) {
+        if (argc != 9) die("genm <start> <seed> <beta> <eps> <utype> <stype> <nsweeps>");
+        int start = atoi(argv[2]), seed = atoi(argv[3]), utype = atoi(argv[6]), stype = atoi(argv[7]);
+        int nsw = atoi(argv[8]);
+        runParams.beta = atof(argv[4]);
+        runParams.eps = atof(argv[5]);
+        rlxd_init(2, seed);
+        setup(start);
+        for (int n = 0; n < nsw; n++) {
+            gaugefieldUpdate(n + 1, 1, utype, stype);
+            printf("RESULT plaq %d %.17g\n", n + 1, plaquette());
+        }
         return 0;
     }
 
@@ -327,6 +346,36 @@ int main(int argc, char *argv[])
             printf("RESULT hb %d %.17g %.17g\n", s, acc / (double)(VOL * DIM), plaquette());
         }
         writeConfig(argv[7]);
+        return 0;
+    }
+#endif
+
+#ifdef SU2_INJECT
+    /* metroinj <cfg|cold|hot> <seed> <beta> <eps> <sweep0> <nsweeps> <out.cfg>: checkerboard sweeps
+     * (dir-major, even then odd parity) of the reference's own localMetropolisUpdate(n, dir, 1)
+     * (metro.c:78-109) on Philox uniforms, then the whole-field reprojection (update.c:166) */
+    if (strcmp(cmd, "metroinj") == 0) {
+        if (argc != 9) die("metroinj <cfg> <seed> <beta> <eps> <sweep0> <nsweeps> <out>");
+        load_or_start(argv[2]);
+        inject_set_seed((uint64_t)strtoull(argv[3], NULL, 0));
+        inject_set_metro(1);
+        runParams.beta = atof(argv[4]);
+        runParams.eps = atof(argv[5]);
+        uint32_t sweep0 = (uint32_t)strtoul(argv[6], NULL, 0);
+        int nsw = atoi(argv[7]);
+        for (int s = 0; s < nsw; s++) {
+            double acc = 0.0;
+            for (int dir = 0; dir < DIM; dir++)
+                for (int p = 0; p < 2; p++)
+                    for (uint64_t n = 0; n < VOL; n++) {
+                        if (site_parity(n) != p) continue;
+                        inject_set_link((uint32_t)n, (uint32_t)dir, sweep0 + (uint32_t)s);
+                        acc += localMetropolisUpdate(n, dir, 1);
+                    }
+            project_gfield_to_sun(pu);
+            printf("RESULT metro %d %.17g %.17g\n", s, acc / (double)(VOL * DIM), plaquette());
+        }
+        writeConfig(argv[8]);
         return 0;
     }
 #endif

@@ -408,14 +408,14 @@ int su2o_start(const int dims[4], double *U, int mode, uint64_t seed, uint32_t r
  * generateSU2InHeatbath_Improved(), LGT_Code/modules/update/heatbath.c:76-149,
  * with the uniforms drawn from the Philox stream of this link.  Returns 1/trials
  * (0 for the zero-staple fallback), as the reference does. */
-static double hb_link(const lat_t *g, double *U, uint64_t n, int mu, double beta, uint64_t seed, uint32_t sweep,
-                      uint32_t replica)
+static double hb_link_v(const lat_t *g, double *U, uint64_t n, int mu, double beta, uint64_t seed, uint32_t sweep,
+                        uint32_t replica, uint32_t draw_base)
 {
     qd A = staple_update(g, U, n, mu);
     double k = q_norm(A);
     uint32_t w[4];
     if (k <= DBL_EPSILON) {
-        su2_philox_link(seed, (uint32_t)n, sweep, (uint32_t)mu, 1, 1, SU2_STREAM_UPDATE, replica, w);
+        su2_philox_link(seed, (uint32_t)n, sweep, (uint32_t)mu, draw_base | 1u, 1, SU2_STREAM_UPDATE, replica, w);
         double r[3] = {philox_u01_f64(w[0]), philox_u01_f64(w[1]), philox_u01_f64(w[2])};
         st(U, n, mu, q_project(ref_random_link(r)));
         return 0.0;
@@ -425,7 +425,7 @@ static double hb_link(const lat_t *g, double *U, uint64_t n, int mu, double beta
     double alpha = k * beta, delta;
     uint32_t trial = 0;
     for (;;) {
-        su2_philox_link(seed, (uint32_t)n, sweep, (uint32_t)mu, trial, 0, SU2_STREAM_UPDATE, replica, w);
+        su2_philox_link(seed, (uint32_t)n, sweep, (uint32_t)mu, draw_base | trial, 0, SU2_STREAM_UPDATE, replica, w);
         trial++;
         double u0 = philox_u01_f64(w[0]), u1 = philox_u01_f64(w[1]);
         double u2 = philox_u01_f64(w[2]), u3 = philox_u01_f64(w[3]);
@@ -434,7 +434,7 @@ static double hb_link(const lat_t *g, double *U, uint64_t n, int mu, double beta
         delta = X2 + X1 * (c * c);
         if (u3 * u3 <= 1.0 - 0.5 * delta) break;
     }
-    su2_philox_link(seed, (uint32_t)n, sweep, (uint32_t)mu, 0, 1, SU2_STREAM_UPDATE, replica, w);
+    su2_philox_link(seed, (uint32_t)n, sweep, (uint32_t)mu, draw_base, 1, SU2_STREAM_UPDATE, replica, w);
     double phi = 2.0 * kPi * philox_u01_f64(w[0]);
     double theta = acos(1.0 - 2.0 * philox_u01_f64(w[1]));
     qd X;
@@ -445,6 +445,62 @@ static double hb_link(const lat_t *g, double *U, uint64_t n, int mu, double beta
     X.c[3] = len * cos(theta);
     st(U, n, mu, q_project(q_mul_nd(X, V)));
     return 1.0 / (double)trial;
+}
+
+static double hb_link(const lat_t *g, double *U, uint64_t n, int mu, double beta, uint64_t seed, uint32_t sweep,
+                      uint32_t replica)
+{
+    return hb_link_v(g, U, n, mu, beta, seed, sweep, replica, 0u);
+}
+
+/* localMetropolisUpdate(n, dir, m) (LGT_Code/modules/update/metro.c:78-109) on Philox draws: hit i
+ * takes one block w of stream SU2_STREAM_METRO with draw index i; w[0..2] are the three uniforms of
+ * proposeNewLink (X_j = 1 - 2 r_j, metro.c:65-76), w[3] the acceptance uniform.  The proposal is
+ * expx(eps, X, u) (exp_fct.c:137-151): U' = E U with E = ((1 - z), eps X) / (1 + z),
+ * z = eps^2 |X|^2 / 4.  Returns the number of accepted hits. */
+static int metro_link(const lat_t *g, double *U, uint64_t n, int mu, double beta, double eps, int hits,
+                      uint64_t seed, uint32_t sweep, uint32_t replica)
+{
+    const qd stap = staple_update(g, U, n, mu);
+    qd u = ld(U, n, mu);
+    int iac = 0;
+    for (int i = 0; i < hits; ++i) {
+        const double lpl_old = 2.0 * q_mul(u, stap).c[0];
+        uint32_t w[4];
+        su2_philox_link(seed, (uint32_t)n, sweep, (uint32_t)mu, (uint32_t)i, 0, SU2_STREAM_METRO, replica, w);
+        double X[3];
+        for (int j = 0; j < 3; ++j) X[j] = 1.0 - 2.0 * philox_u01_f64(w[j]);
+        double zw = eps * eps * (X[0] * X[0] + X[1] * X[1] + X[2] * X[2]) / 4.0;
+        qd e;
+        e.c[0] = 1.0 - zw;
+        zw = 1.0 / (1.0 + zw);
+        e.c[0] *= zw;
+        for (int j = 0; j < 3; ++j) e.c[j + 1] = zw * eps * X[j];
+        const qd prop = q_mul(e, u);
+        const double lpl = 2.0 * q_mul(prop, stap).c[0];
+        if (philox_u01_f64(w[3]) <= exp(beta * (lpl - lpl_old) / 2.0)) {
+            u = prop;
+            iac++;
+        }
+    }
+    st(U, n, mu, q_project(u));
+    return iac;
+}
+
+/* Times a site is drawn when V sites are drawn with replacement (the random sweep of
+ * gaugefieldUpdate, update.c:126-136): Binomial(V, 1/V) by inverse CDF on one uniform. */
+static int visit_count(uint32_t w, uint64_t V)
+{
+    const double u = philox_u01_f64(w), v = (double)V;
+    const double p0 = exp(v * log1p(-1.0 / v));
+    double p = p0, c = p0;
+    int k = 0;
+    while (u > c && k < 32) {
+        p *= (v - k) / ((k + 1) * (v - 1.0));
+        c += p;
+        ++k;
+    }
+    return k;
 }
 
 /* Overrelaxation (no reference counterpart): U' = W^dag U^dag W^dag with W = A/|A|,
@@ -568,5 +624,37 @@ int su2o_reflect(const int dims[4], const double *small, double *U)
             }
         }
     }
+    return 0;
+}
+
+/* One sweep of gaugefieldUpdate(iup, 1, utype, stype) (update.c:102-175) in checkerboard order,
+ * as the library runs it: utype 1 heatbath / 0 Metropolis (`hits` hits per visit, step eps);
+ * stype 0 every link once / 1 a Binomial(V, 1/V) number of visits per site (stream
+ * SU2_STREAM_VISIT, one count per site and sweep).  acc gets the mean acceptance per link visit
+ * over 4 V expected visits. */
+int su2o_visit_sweep(const int dims[4], double *U, int utype, int stype, double beta, double eps, int hits,
+                     uint64_t seed, uint32_t sweep, uint32_t replica, double *acc)
+{
+    lat_t g;
+    if (lat_init(&g, dims)) return -1;
+    double a = 0.0;
+    for (int mu = 0; mu < 4; ++mu)
+        for (int p = 0; p < 2; ++p)
+            for (uint64_t n = 0; n < g.V; ++n) {
+                if (parity(&g, n) != p) continue;
+                int visits = 1;
+                if (stype == 1) {
+                    uint32_t w[4];
+                    su2_philox_link(seed, (uint32_t)n, sweep, 0, 0, 0, SU2_STREAM_VISIT, replica, w);
+                    visits = visit_count(w[0], g.V);
+                }
+                if (utype == 1) {
+                    for (int v = 0; v < visits; ++v)
+                        a += hb_link_v(&g, U, n, mu, beta, seed, sweep, replica, (uint32_t)v << SU2_VISIT_SHIFT);
+                } else if (visits > 0) {
+                    a += (double)metro_link(&g, U, n, mu, beta, eps, visits * hits, seed, sweep, replica) / hits;
+                }
+            }
+    if (acc) *acc = a / (4.0 * (double)g.V);
     return 0;
 }

@@ -40,6 +40,8 @@ def lib():
         L.su2o_link_action.argtypes = [_IP, _DP, _DP]
         L.su2o_kp_samples.argtypes = [ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64, _DP]
         L.su2o_reflect.argtypes = [_IP, _DP, _DP]
+        L.su2o_visit_sweep.argtypes = [_IP, _DP, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, _DP]
         _lib = L
     return _lib
 
@@ -134,6 +136,16 @@ def reflect(dims, small):
     out = np.zeros((int(np.prod(dims)), 4, 4))
     _ok(lib().su2o_reflect(_dims(dims), _dp(small), _dp(out)))
     return out
+
+
+def visit_sweep(dims, U, utype, stype, beta, eps, hits, seed, sweep_index, replica=0):
+    """One gaugefieldUpdate sweep (utype 1 heatbath / 0 Metropolis, stype 0 / 1 random sites) in
+    checkerboard order, in place on U; returns the mean acceptance per link visit."""
+    assert U.dtype == np.float64 and U.flags["C_CONTIGUOUS"]
+    a = ctypes.c_double()
+    _ok(lib().su2o_visit_sweep(_dims(dims), _dp(U), int(utype), int(stype), float(beta), float(eps), int(hits),
+                               int(seed), int(sweep_index), int(replica), ctypes.byref(a)))
+    return a.value
 
 
 def golden():

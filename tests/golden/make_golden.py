@@ -20,6 +20,12 @@ Outputs
                  and written by its writeConfig: sha256 of the link payload (the bytes after
                  the 32-byte header), the header plaquette and the computed one.  Run
                  `make_golden.py --reflect-only` to refresh this part alone.
+  golden.json["metropolis"]  the reference's localMetropolisUpdate (metro.c:78-109) on Philox
+                 uniforms in checkerboard order (cfg_*_metroinj.cfg, acceptance, plaquette), and
+                 the reference's own RANLUX chains at 8^4, beta 3.09 for Metropolis with
+                 sequential and random site order and for heatbath with random order
+                 (gaugefieldUpdate utype/stype, update.c:102-175): plaquette mean, error, tau_int.
+                 `make_golden.py --metro-only` refreshes this part alone.
   kp_improved.dat  the reference's Kennedy-Pendleton sampler histogram at
                  alpha=7 (copied from LGT_Code/main_test/improved.dat; 200 bins
                  of N=1e8 draws; column 2 is count*200/N).
@@ -73,7 +79,43 @@ def reflect_golden(gold):
     gold["reflect"] = out
 
 
+METRO_INJ = {"seed": 777, "beta": 3.09, "eps": 0.5, "sweep0": 3, "sweeps": 2}
+METRO_CHAINS = [(0, 0), (0, 1), (1, 1)]   # (utype, stype)
+METRO_CHAIN = {"dims": [8, 8, 8, 8], "beta": 3.09, "eps": 0.5, "start": 0, "seed": 11, "sweeps": 6000, "therm": 500}
+
+
+def metro_golden(gold):
+    sys.path.insert(0, os.path.dirname(HERE))
+    import _stats
+    out = {"inj": {}, "chains": []}
+    e = METRO_INJ
+    for dims in sorted(LINK_LEVEL):
+        cfg = f"cfg_{dims}_metroinj.cfg"
+        rr = run([harness(dims, True), "metroinj", os.path.join(HERE, f"cfg_{dims}_base.cfg"), str(e["seed"]),
+                  str(e["beta"]), str(e["eps"]), str(e["sweep0"]), str(e["sweeps"]), os.path.join(HERE, cfg)])
+        out["inj"][dims] = dict(e, cfg=cfg, acc=[float(x[1]) for x in rr], plaq=[float(x[2]) for x in rr])
+    c = METRO_CHAIN
+    for utype, stype in METRO_CHAINS:
+        rr = run([harness("8x8x8x8"), "genm", str(c["start"]), str(c["seed"]), str(c["beta"]), str(c["eps"]),
+                  str(utype), str(stype), str(c["sweeps"])])
+        plaq = [float(x[1]) for x in rr]
+        m, err, tau = _stats.mean_err(plaq[c["therm"]:])
+        out["chains"].append(dict(c, utype=utype, stype=stype, mean=m, err=err, tau_int=tau))
+    out["chain_note"] = ("reference gaugefieldUpdate with RANLUX; plaquette after every sweep; "
+                         "the first `therm` sweeps discarded; errors by the t_int.c Gamma method")
+    gold["metropolis"] = out
+
+
 def main():
+    if "--metro-only" in sys.argv:
+        path = os.path.join(HERE, "golden.json")
+        with open(path) as f:
+            gold = json.load(f)
+        metro_golden(gold)
+        with open(path, "w") as f:
+            json.dump(gold, f, indent=1)
+        print("updated", path)
+        return 0
     if "--reflect-only" in sys.argv:
         path = os.path.join(HERE, "golden.json")
         with open(path) as f:
@@ -165,6 +207,7 @@ def main():
     gold["chain_8x8x8x8_b3.09"] = chain
 
     reflect_golden(gold)
+    metro_golden(gold)
     shutil.copyfile(os.path.join(REF, "LGT_Code", "main_test", "improved.dat"), os.path.join(HERE, "kp_improved.dat"))
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(gold, f, indent=1)

@@ -153,3 +153,18 @@ def test_reflection_matches_reference(golden, big):
     assert hashlib.sha256(U.astype("<f8").tobytes()).hexdigest() == g["payload_sha256"]
     p = O.plaquette(dims, U)
     assert abs(p - g["plaq"]) <= 1e-14 and abs(p - plaq0) <= 1e-13
+
+
+@pytest.mark.parametrize("lat", ["4x4x4x4", "6x4x4x8"])
+def test_metropolis_matches_reference_on_injected_uniforms(golden, lat):
+    """localMetropolisUpdate (metro.c:78-109) of the reference, fed the Philox uniforms of each link,
+    against the oracle's Metropolis sweep: identical links and acceptance."""
+    e = golden["metropolis"]["inj"][lat]
+    dims, _, U = O.golden_config(f"cfg_{lat}_base.cfg")
+    _, _, R = O.golden_config(e["cfg"])
+    W = U.copy()
+    for s in range(e["sweeps"]):
+        acc = O.visit_sweep(dims, W, 0, 0, e["beta"], e["eps"], 1, e["seed"], e["sweep0"] + s)
+        assert acc == e["acc"][s]
+    assert np.max(np.abs(W - R)) <= 1e-14
+    assert abs(O.plaquette(dims, W) - e["plaq"][-1]) <= 1e-14
