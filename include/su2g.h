@@ -160,6 +160,26 @@ int su2g_measure(su2g_lattice *h, const su2g_meas_spec *spec, double *q, double 
 /* Free the measurement graph and its two field copies (also freed by su2g_destroy). */
 int su2g_measure_release(su2g_lattice *h);
 
+/* ---- the reference's analysis tools on the device.  Inputs may be host or device memory;
+ * outputs are host memory; the calls synchronise `device` and report failures through
+ * su2g_last_error(NULL).
+ * su2g_stats_tau_int: LGT_Code/Autocorrelation/t_int.c:24-74 for n_series series of length n,
+ * element i of series s at data[i * stride_i + s * stride_s]: out[4 s + {0,1,2,3}] = mean,
+ * integrated autocorrelation time tau (Gamma(k) with separate window means, summed up to the
+ * first negative lag), naive error sqrt(Gamma(0)/(n-1)) and error sqrt(2 tau) x naive; resolved[s]
+ * (may be NULL) = 1 when ceil(100 tau) <= n, the tool's condition for a trustworthy tau (t_int.c:65-69).
+ * The sums run in the tool's order, so the results equal its arithmetic. */
+int su2g_stats_tau_int(const double *data, int64_t n, int32_t n_series, int64_t stride_i, int64_t stride_s,
+                       int32_t device, double *out, int32_t *resolved);
+/* su2g_stats_veff: the block jackknife of Analysis/static potential/static_potential.py:28-146
+ * on w[c][r][t] = W(R_r, T_t) of configuration c (n_conf x n_r x n_t): n_bins blocks of
+ * n_conf / n_bins configurations, veff[r][t] = log(W(T_t)/W(T_t+1)) bias corrected and its
+ * jackknife error veff_err (n_r x (n_t - 1)), v[r] = the weighted constant fit of veff over
+ * t in [t_fit_start[r], t_fit_end[r]) (indices into veff), bias corrected, and its jackknife error. */
+int su2g_stats_veff(const double *w, int32_t n_conf, int32_t n_r, int32_t n_t, int32_t n_bins,
+                    const int32_t *t_fit_start, const int32_t *t_fit_end, int32_t device, double *veff,
+                    double *veff_err, double *v, double *v_err);
+
 /* ---- the driver loop of LGT_Code/main/qcd.c:55-60 (gaugefieldUpdate, then plaquette) as one
  * replayed CUDA graph.  Runs n_blocks blocks of [meas_every x (n_hb heatbath + n_or overrelaxation
  * sweeps), plaquette].  The block is captured on first use and replayed; it is captured again
@@ -218,6 +238,11 @@ int su2g_batch_run(su2g_batch *b, int32_t n_sweeps, int32_t n_hb, int32_t n_or, 
                    double *plaq_trace, double *ms);
 /* Times the sweep for each candidate CTA size and keeps the fastest (the fields are restored). */
 int su2g_batch_autotune(su2g_batch *b, int32_t n_hb, int32_t n_or, int32_t *block_out);
+/* The integrated autocorrelation analysis of LGT_Code/Autocorrelation/t_int.c (see
+ * su2g_stats_tau_int) of every replica's plaquette trace from the last su2g_batch_run, on the
+ * device, the first `skip` measurements left out: out[4 r + {0,1,2,3}] = mean, tau_int, naive
+ * error, error of replica r; resolved[r] (may be NULL) = 1 when 100 tau_int <= the series length. */
+int su2g_batch_tau_int(su2g_batch *b, int32_t skip, double *out, int32_t *resolved);
 int su2g_batch_download(su2g_batch *b, int32_t r, double *links);
 int su2g_batch_upload(su2g_batch *b, int32_t r, const double *links);
 

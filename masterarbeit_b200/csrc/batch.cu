@@ -49,6 +49,7 @@ struct su2g_batch {
     unsigned* d_status = nullptr;
     double* d_trace = nullptr;
     size_t trace_cap = 0;
+    int trace_rows = 0;                            // measurements in the trace of the last run
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int g_hb = -1, g_or = -1, g_meas = -1, g_every = -1, g_block = -1;
@@ -473,9 +474,37 @@ extern "C" int su2g_batch_run(su2g_batch* b, int32_t n_sweeps, int32_t n_hb, int
         *ms = f;
     }
     if ((rc = check_status(b))) return rc;
+    b->trace_rows = meas ? nblocks : 0;
     if (meas && plaq_trace && nblocks > 0)
         rc = bcuda(b, cudaMemcpy(plaq_trace, b->d_trace, (size_t)nblocks * b->n * sizeof(double), cudaMemcpyDeviceToHost),
                    "copying the trace");
+    return rc;
+}
+
+extern "C" int su2g_batch_tau_int(su2g_batch* b, int32_t skip, double* out, int32_t* resolved)
+{
+    if (!b) return set_error(nullptr, SU2G_EINVAL, "su2g_batch_tau_int: null batch");
+    if (!out || skip < 0 || b->trace_rows - skip < 2)
+        return berr(b, SU2G_EINVAL, "su2g_batch_tau_int: needs an output and at least 2 measurements after skip "
+                                    "(trace has %d)", b->trace_rows);
+    cudaSetDevice(b->device);
+    double* d_out = nullptr;
+    int* d_res = nullptr;
+    int rc = bcuda(b, cudaMalloc(&d_out, 4 * (size_t)b->n * sizeof(double)), "allocating results");
+    if (!rc) rc = bcuda(b, cudaMalloc(&d_res, (size_t)b->n * sizeof(int)), "allocating results");
+    // trace[meas][replica]: series r has stride n and starts at row `skip`
+    if (!rc && tau_int_enqueue(b->d_trace + (size_t)skip * b->n, b->trace_rows - skip, b->n, 1, b->n, b->stream, d_out,
+                               d_res))
+        rc = berr(b, SU2G_ECUDA, "su2g_batch_tau_int: %s", su2g_last_error(nullptr));
+    if (!rc)
+        rc = bcuda(b, cudaMemcpyAsync(out, d_out, 4 * (size_t)b->n * sizeof(double), cudaMemcpyDeviceToHost, b->stream),
+                   "copying results");
+    if (!rc && resolved)
+        rc = bcuda(b, cudaMemcpyAsync(resolved, d_res, (size_t)b->n * sizeof(int), cudaMemcpyDeviceToHost, b->stream),
+                   "copying results");
+    if (!rc) rc = bcuda(b, cudaStreamSynchronize(b->stream), "analysing the trace");
+    cudaFree(d_out);
+    cudaFree(d_res);
     return rc;
 }
 

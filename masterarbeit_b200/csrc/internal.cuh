@@ -182,6 +182,10 @@ int qtop_enqueue(su2g_lattice* h, void* const dirs[4], int out_off);
 int ensure_aos(su2g_lattice* h);
 int aos_to_field(su2g_lattice* h, const double* d_src, size_t n0, int count);
 int field_to_aos(su2g_lattice* h, double* d_dst, size_t n0, int count);
+// t_int.c on n_series device series (element i of series s at d_x[i*si + s*ss]); d_out gets
+// {mean, tau_int, naive error, error} per series, d_resolved 100 tau <= n (stats.cu).
+int tau_int_enqueue(const double* d_x, long long n, long long si, long long ss, int n_series, cudaStream_t stream,
+                    double* d_out, int* d_resolved);
 // Destroy the captured su2g_measure graph, if any.
 void release_meas_graph(su2g_lattice* h);
 // Destroy the captured su2g_graph_run block, if any.

@@ -94,6 +94,11 @@ _SIGS = {
     "su2g_measure_release": (ctypes.c_int, [_P]),
     "su2g_gauge_update": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                          ctypes.c_int32, _DP]),
+    "su2g_stats_tau_int": (ctypes.c_int, [_DP, ctypes.c_int64, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
+                                          ctypes.c_int32, _DP, _I32P]),
+    "su2g_stats_veff": (ctypes.c_int, [_DP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _I32P,
+                                       _I32P, ctypes.c_int32, _DP, _DP, _DP, _DP]),
+    "su2g_batch_tau_int": (ctypes.c_int, [_P, ctypes.c_int32, _DP, _I32P]),
     "su2g_plaquette": (ctypes.c_int, [_P, _DP]),
     "su2g_ape": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32]),
     "su2g_wilson": (ctypes.c_int, [_P, _I32P, _I32P, ctypes.c_int32, _DP]),
@@ -393,6 +398,39 @@ class Lattice:
         return out
 
 
+def stats_tau_int(series, device=0):
+    """t_int.c on the device for each column of `series` ([n] or [n, n_series]): returns
+    (array [n_series, 4] of mean, tau_int, naive error, error; resolved flags)."""
+    lib = load()
+    x = np.ascontiguousarray(series, dtype=np.float64)
+    n, ns = (x.shape[0], 1) if x.ndim == 1 else x.shape
+    out = np.zeros((ns, 4))
+    res = np.zeros(ns, dtype=np.int32)
+    rc = lib.su2g_stats_tau_int(x.ctypes.data_as(_DP), n, ns, ns, 1, int(device), out.ctypes.data_as(_DP),
+                                res.ctypes.data_as(_I32P))
+    if rc:
+        raise Su2gError(rc, lib.su2g_last_error(None).decode())
+    return out, res.astype(bool)
+
+
+def stats_veff(w, n_bins, t_fit_start, t_fit_end, device=0):
+    """static_potential.py's jackknife on the device; w[c][r][t] = W(R_r, T_t).  Returns
+    (veff, veff_err) [n_r][n_t - 1] and (v, v_err) [n_r]."""
+    lib = load()
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    n_conf, n_r, n_t = w.shape
+    ve, er = np.zeros((n_r, n_t - 1)), np.zeros((n_r, n_t - 1))
+    v, verr = np.zeros(n_r), np.zeros(n_r)
+    t0 = (ctypes.c_int32 * n_r)(*[int(x) for x in t_fit_start])
+    t1 = (ctypes.c_int32 * n_r)(*[int(x) for x in t_fit_end])
+    rc = lib.su2g_stats_veff(w.ctypes.data_as(_DP), n_conf, n_r, n_t, int(n_bins), t0, t1, int(device),
+                             ve.ctypes.data_as(_DP), er.ctypes.data_as(_DP), v.ctypes.data_as(_DP),
+                             verr.ctypes.data_as(_DP))
+    if rc:
+        raise Su2gError(rc, lib.su2g_last_error(None).decode())
+    return ve, er, v, verr
+
+
 class Batch:
     """Many independent replicas (extents, beta, seed, start per replica) driven together."""
 
@@ -441,6 +479,14 @@ class Batch:
         self._check(self.lib.su2g_batch_run(self.h, int(n_sweeps), int(n_hb), int(n_or), int(meas_every),
                                             _as_dp(trace) if trace is not None else None, ctypes.byref(ms)))
         return trace, ms.value
+
+    def tau_int(self, skip=0):
+        """t_int.c of every replica's plaquette trace from the last run, on the device: (array
+        [n, 4] of mean, tau_int, naive error, error; resolved flags)."""
+        out = np.zeros((self.n, 4))
+        res = np.zeros(self.n, dtype=np.int32)
+        self._check(self.lib.su2g_batch_tau_int(self.h, int(skip), out.ctypes.data_as(_DP), res.ctypes.data_as(_I32P)))
+        return out, res.astype(bool)
 
     def autotune(self, n_hb=1, n_or=4):
         b = ctypes.c_int32()

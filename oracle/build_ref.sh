@@ -39,6 +39,12 @@ MODULES=(
 
 CFLAGS="-O3 -w -mcmodel=large"
 
+# the reference's stand-alone autocorrelation tool (LGT_Code/Autocorrelation/t_int.c), unmodified
+mkdir -p "$HERE/_ref"
+if [ ! -x "$HERE/_ref/t_int" ] || [ "$LGT/Autocorrelation/t_int.c" -nt "$HERE/_ref/t_int" ]; then
+    gcc -O2 -w "$LGT/Autocorrelation/t_int.c" -lm -o "$HERE/_ref/t_int"
+fi
+
 for spec in "${DIMS[@]}"; do
     IFS=x read -r LT L1 L2 L3 <<<"$spec"
     OUT="$HERE/_ref/$spec"

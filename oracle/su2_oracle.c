@@ -658,3 +658,109 @@ int su2o_visit_sweep(const int dims[4], double *U, int utype, int stype, double 
     if (acc) *acc = a / (4.0 * (double)g.V);
     return 0;
 }
+
+/* ------------------------------------------------------------- statistics --- */
+
+/* LGT_Code/Autocorrelation/t_int.c:24-74 for one series x[i * stride], i < n: out = {mean,
+ * integrated autocorrelation time (integratedAutocorrelationTime, :44-55), naive error (:58-60),
+ * error = sqrt(2 tau) naive (:71)}; returns 1 when ceil(100 tau) <= n (:65-69), else 0.  The sums
+ * run in the reference's order. */
+static double ts_avg(const double *x, int64_t stride, int64_t a, int64_t b)
+{
+    double s = 0.0;
+    for (int64_t i = a; i < b; ++i) s += x[i * stride];
+    return s / (double)(b - a);
+}
+
+static double ts_gamma(const double *x, int64_t stride, int64_t n, int64_t k)
+{
+    const double a0 = ts_avg(x, stride, 0, n - k), ak = ts_avg(x, stride, k, n);
+    double c = 0.0;
+    for (int64_t i = 0; i < n - k; ++i) c += (x[i * stride] - a0) * (x[(i + k) * stride] - ak);
+    return c / (double)(n - k);
+}
+
+int su2o_tau_int(const double *x, int64_t n, int64_t stride, double out[4])
+{
+    const double g0 = ts_gamma(x, stride, n, 0);
+    double t = 0.5 * g0;
+    for (int64_t k = 1; k < n; ++k) {
+        const double gk = ts_gamma(x, stride, n, k);
+        if (gk < 0.0) break;
+        t += gk;
+    }
+    const double tau = t / g0, naive = sqrt(g0 / (double)(n - 1));
+    out[0] = ts_avg(x, stride, 0, n);
+    out[1] = tau;
+    out[2] = naive;
+    out[3] = sqrt(2.0 * tau) * naive;
+    return (int64_t)ceil(100.0 * tau) <= n;
+}
+
+/* The jackknife effective potential of Analysis/static potential/static_potential.py:80-146.
+ * w[c][r][t] (n_conf x n_r x n_t) are W(R_r, T_t) per configuration.  With B = n_bins blocks of
+ * L = n_conf / B configurations (block k = [kL, (k+1)L); the n_conf - B L last ones are never
+ * left out):
+ *   Wbar, Wbar_k       means over all configurations and over all but block k (:80-86);
+ *   V_eff(r,t)         log(Wbar(t) / Wbar(t+1)) and V_eff_k likewise (:90-97);
+ *   err(r,t)           sqrt((B-1)/B sum_k (V_eff_k - V_eff)^2) (:100-107);
+ *   veff(r,t)          V_eff - (B-1)(mean_k V_eff_k - V_eff) (bias corrected, :110-113);
+ *   fit_k(r)           sum_t V_eff_k / err^2 / sum_t 1/err^2 over t in [t0(r), t1(r)) (:28-42, :117-127);
+ *   v(r)               the same fit of the corrected veff (:129-132);
+ *   v_err(r)           sqrt((B-1)/B sum_k (fit_k - v)^2) (:135-141);
+ *   v(r)               corrected: v - (B-1)(mean_k fit_k - v) (:143-145).
+ * veff, veff_err: n_r x (n_t - 1).  Sums run in index order. */
+int su2o_veff(const double *w, int n_conf, int n_r, int n_t, int n_bins, const int *t0, const int *t1, double *veff,
+              double *veff_err, double *v, double *v_err)
+{
+    const int B = n_bins, L = n_conf / B, nt1 = n_t - 1;
+    if (B < 2 || L < 1 || n_t < 2) return -1;
+    double *wbar = malloc(sizeof(double) * n_r * n_t * (B + 1));
+    double *vj = malloc(sizeof(double) * n_r * nt1 * B);
+    if (!wbar || !vj) return -1;
+    for (int r = 0; r < n_r; ++r)
+        for (int t = 0; t < n_t; ++t) {
+            double all = 0.0;
+            for (int c = 0; c < n_conf; ++c) all += w[((size_t)c * n_r + r) * n_t + t];
+            double *wb = wbar + ((size_t)r * n_t + t) * (B + 1);
+            wb[0] = all / n_conf;
+            for (int k = 0; k < B; ++k) {
+                double blk = 0.0;
+                for (int c = k * L; c < (k + 1) * L; ++c) blk += w[((size_t)c * n_r + r) * n_t + t];
+                wb[1 + k] = (all - blk) / (n_conf - L);
+            }
+        }
+    for (int r = 0; r < n_r; ++r)
+        for (int t = 0; t < nt1; ++t) {
+            const double *a = wbar + ((size_t)r * n_t + t) * (B + 1), *b = a + (B + 1);
+            const double full = log(a[0] / b[0]);
+            double s2 = 0.0, sm = 0.0;
+            for (int k = 0; k < B; ++k) {
+                const double e = log(a[1 + k] / b[1 + k]);
+                vj[((size_t)r * nt1 + t) * B + k] = e;
+                s2 += (e - full) * (e - full);
+                sm += e;
+            }
+            veff_err[(size_t)r * nt1 + t] = sqrt((double)(B - 1) / B * s2);
+            veff[(size_t)r * nt1 + t] = full - (B - 1) * (sm / B - full);
+        }
+    for (int r = 0; r < n_r; ++r) {
+        const double *ve = veff + (size_t)r * nt1, *er = veff_err + (size_t)r * nt1;
+        double sig = 0.0;
+        for (int t = t0[r]; t < t1[r]; ++t) sig += 1.0 / (er[t] * er[t]);
+        double a = 0.0;
+        for (int t = t0[r]; t < t1[r]; ++t) a += ve[t] / (sig * er[t] * er[t]);
+        double s2 = 0.0, sm = 0.0;
+        for (int k = 0; k < B; ++k) {
+            double f = 0.0;
+            for (int t = t0[r]; t < t1[r]; ++t) f += vj[((size_t)r * nt1 + t) * B + k] / (sig * er[t] * er[t]);
+            s2 += (f - a) * (f - a);
+            sm += f;
+        }
+        v_err[r] = sqrt((double)(B - 1) / B * s2);
+        v[r] = a - (B - 1) * (sm / B - a);
+    }
+    free(wbar);
+    free(vj);
+    return 0;
+}

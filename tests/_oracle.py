@@ -40,6 +40,9 @@ def lib():
         L.su2o_link_action.argtypes = [_IP, _DP, _DP]
         L.su2o_kp_samples.argtypes = [ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64, _DP]
         L.su2o_reflect.argtypes = [_IP, _DP, _DP]
+        L.su2o_tau_int.argtypes = [_DP, ctypes.c_int64, ctypes.c_int64, _DP]
+        L.su2o_veff.argtypes = [_DP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _IP, _IP, _DP, _DP, _DP,
+                                _DP]
         L.su2o_visit_sweep.argtypes = [_IP, _DP, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, _DP]
         _lib = L
@@ -146,6 +149,25 @@ def visit_sweep(dims, U, utype, stype, beta, eps, hits, seed, sweep_index, repli
     _ok(lib().su2o_visit_sweep(_dims(dims), _dp(U), int(utype), int(stype), float(beta), float(eps), int(hits),
                                int(seed), int(sweep_index), int(replica), ctypes.byref(a)))
     return a.value
+
+
+def tau_int(x):
+    """t_int.c on one series: ((mean, tau_int, naive error, error), resolved)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros(4)
+    ok = lib().su2o_tau_int(_dp(x), len(x), 1, _dp(out))
+    return out, bool(ok)
+
+
+def veff(w, n_bins, t0, t1):
+    """static_potential.py's jackknife: (veff, veff_err) [n_r][n_t-1] and (v, v_err) [n_r]."""
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    n_conf, n_r, n_t = w.shape
+    ve, er = np.zeros((n_r, n_t - 1)), np.zeros((n_r, n_t - 1))
+    v, ve_r = np.zeros(n_r), np.zeros(n_r)
+    a0, a1 = (ctypes.c_int * n_r)(*t0), (ctypes.c_int * n_r)(*t1)
+    _ok(lib().su2o_veff(_dp(w), n_conf, n_r, n_t, n_bins, a0, a1, _dp(ve), _dp(er), _dp(v), _dp(ve_r)))
+    return ve, er, v, ve_r
 
 
 def golden():

@@ -26,6 +26,12 @@ Outputs
                  sequential and random site order and for heatbath with random order
                  (gaugefieldUpdate utype/stype, update.c:102-175): plaquette mean, error, tau_int.
                  `make_golden.py --metro-only` refreshes this part alone.
+  golden.json["stats"]  outputs of the reference's analysis tools on synthetic data that
+                 tests/_stats.py regenerates from the recorded seeds:
+                 LGT_Code/Autocorrelation/t_int.c (compiled by oracle/build_ref.sh) on two
+                 AR(1) series, and Analysis/static potential/static_potential.py (run here,
+                 its plotting module replaced by a no-op stand-in, matplotlib being absent) on
+                 1000 configurations of W(R<=12, T<=20).  `make_golden.py --stats-only`.
   kp_improved.dat  the reference's Kennedy-Pendleton sampler histogram at
                  alpha=7 (copied from LGT_Code/main_test/improved.dat; 200 bins
                  of N=1e8 draws; column 2 is count*200/N).
@@ -36,6 +42,8 @@ import os
 import shutil
 import subprocess
 import sys
+
+import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
@@ -106,7 +114,86 @@ def metro_golden(gold):
     gold["metropolis"] = out
 
 
+class _NoPlot:
+    """Stand-in for matplotlib: every attribute, call and index returns the stand-in."""
+
+    def __getattr__(self, name):
+        return self
+
+    def __call__(self, *a, **k):
+        return self
+
+    def __getitem__(self, i):
+        return self
+
+    def __iter__(self):
+        return iter((self, self))
+
+
+def stats_golden(gold):
+    import contextlib
+    import io
+    import runpy
+    import tempfile
+    import types
+
+    sys.path.insert(0, os.path.dirname(HERE))
+    import _stats
+    out = {"t_int": [], "veff": {}}
+    for seed, phi, n in _stats.AR1_SERIES:
+        x = _stats.ar1_series(seed, phi, n)
+        with tempfile.TemporaryDirectory() as d:
+            f = os.path.join(d, "series.txt")
+            np.savetxt(f, x, fmt="%.17g")
+            txt = subprocess.run([os.path.join(REPO, "oracle", "_ref", "t_int"), f], check=True, capture_output=True,
+                                 text=True).stdout
+        m = txt.split("\n")[1].split()
+        out["t_int"].append({"seed": seed, "phi": phi, "n": n, "sha256": hashlib.sha256(x.tobytes()).hexdigest(),
+                             "mean": float(m[0]), "err": float(m[2]), "two_tau": float(m[6])})
+    w = _stats.veff_data()
+    script = os.path.join(REF, "Analysis", "static potential", "static_potential.py")
+    stub = types.ModuleType("matplotlib")
+    stub.pyplot = _NoPlot()
+    saved = {k: sys.modules.get(k) for k in ("matplotlib", "matplotlib.pyplot")}
+    sys.modules["matplotlib"], sys.modules["matplotlib.pyplot"] = stub, stub.pyplot
+    cwd = os.getcwd()
+    try:
+        with tempfile.TemporaryDirectory() as d:
+            with open(os.path.join(d, "24x24x24x24_SU2_b3.09_NAPE_400.meas"), "w") as f:
+                f.write(_stats.veff_meas_text(w))
+            os.chdir(d)
+            buf = io.StringIO()
+            with contextlib.redirect_stdout(buf):
+                runpy.run_path(script, run_name="__main__")
+    finally:
+        os.chdir(cwd)
+        for k, v in saved.items():
+            if v is None:
+                sys.modules.pop(k, None)
+            else:
+                sys.modules[k] = v
+    veff, vr = [], []
+    for line in buf.getvalue().splitlines():
+        f = line.split("\t")
+        if len(f) == 3:
+            veff.append([int(f[0]), int(f[1]), float(f[2])])
+        elif len(f) == 4:
+            vr.append([int(f[0]), float(f[2]), float(f[3])])
+    out["veff"] = {"sha256": hashlib.sha256(w.tobytes()).hexdigest(), "veff": veff, "v": vr,
+                   "n_bins": 20, "t_fit_start": [7] * 9 + [8] * 3, "t_fit_end": [17] * 12}
+    gold["stats"] = out
+
+
 def main():
+    if "--stats-only" in sys.argv:
+        path = os.path.join(HERE, "golden.json")
+        with open(path) as f:
+            gold = json.load(f)
+        stats_golden(gold)
+        with open(path, "w") as f:
+            json.dump(gold, f, indent=1)
+        print("updated", path)
+        return 0
     if "--metro-only" in sys.argv:
         path = os.path.join(HERE, "golden.json")
         with open(path) as f:
@@ -208,6 +295,7 @@ def main():
 
     reflect_golden(gold)
     metro_golden(gold)
+    stats_golden(gold)
     shutil.copyfile(os.path.join(REF, "LGT_Code", "main_test", "improved.dat"), os.path.join(HERE, "kp_improved.dat"))
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(gold, f, indent=1)

@@ -168,3 +168,39 @@ def test_metropolis_matches_reference_on_injected_uniforms(golden, lat):
         assert acc == e["acc"][s]
     assert np.max(np.abs(W - R)) <= 1e-14
     assert abs(O.plaquette(dims, W) - e["plaq"][-1]) <= 1e-14
+
+
+def test_tau_int_matches_reference_tool(golden):
+    """LGT_Code/Autocorrelation/t_int.c, run by the golden generator on two AR(1) series, against the
+    oracle's restatement (printed to 6 decimals there) and the tests' own Python restatement."""
+    import hashlib
+
+    import _stats
+
+    for g in golden["stats"]["t_int"]:
+        x = _stats.ar1_series(g["seed"], g["phi"], g["n"])
+        assert hashlib.sha256(x.tobytes()).hexdigest() == g["sha256"]
+        (mean, tau, naive, err), ok = O.tau_int(x)
+        assert ok
+        assert abs(mean - g["mean"]) <= 6e-7 and abs(err - g["err"]) <= 6e-7 and abs(2 * tau - g["two_tau"]) <= 6e-7
+        m2, e2, t2 = _stats.mean_err(x)
+        assert abs(m2 - mean) <= 1e-12 and abs(t2 - tau) <= 1e-9 * tau and abs(e2 - err) <= 1e-9 * err
+
+
+def test_veff_matches_reference_script(golden):
+    """static_potential.py (jackknife effective potential, bias-corrected plateau fits), run by the
+    golden generator on 1000 synthetic configurations, against the oracle's restatement."""
+    import hashlib
+
+    import _stats
+
+    g = golden["stats"]["veff"]
+    w = _stats.veff_data()
+    assert hashlib.sha256(w.tobytes()).hexdigest() == g["sha256"]
+    # fit ranges are indices into V_eff(T), T = index + 1, as in the script
+    ve, er, v, verr = O.veff(w, g["n_bins"], g["t_fit_start"], g["t_fit_end"])
+    for r, t, val in g["veff"]:
+        assert abs(ve[r - 1, t - 1] - val) <= 6e-7 * abs(val) + 1e-12, (r, t, ve[r - 1, t - 1], val)
+    for r, val, sig in g["v"]:
+        assert abs(v[r - 1] - val) <= 6e-7 * abs(val)
+        assert abs(verr[r - 1] - sig) <= 6e-7 * abs(sig)
