@@ -219,6 +219,39 @@ def cpu_reference_rate(dims, reps, warm, sites, procs=None):
     }
 
 
+def cpu_reference_kernels(gpu, dims, ref_dims=(24, 24, 24, 24)):
+    """The reference's own APE_all / APE spatial steps, W(R<=9, T<=9) set and Q, one process each on
+    one core, at `ref_dims` (timed by the reference's getTime), scaled per site to `dims`, beside the
+    GPU figures of the same run.  The processes run concurrently (one core each)."""
+    exe = ref_harness(ref_dims)
+    if not exe:
+        return None
+    jobs = {"ape_all": ["bench_ape", "all", "0.5", "3"], "ape_spatial": ["bench_ape", "spatial", "0.5", "3"],
+            "wilson_R9T9": ["bench_wil", "9", "9", "1"], "qtop": ["bench_qtop", "1"]}
+    ps = {k: subprocess.Popen([exe] + a, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, cwd="/tmp")
+          for k, a in jobs.items()}
+    scale = math.prod(dims) / math.prod(ref_dims)
+    out = {"ref_dims": list(ref_dims), "note": "single-core reference time per unit at ref_dims, scaled by the "
+                                               "site count to the workload; GPU rates from this run"}
+    gpu_rate = {"ape_all": "ape_all_steps_per_s", "ape_spatial": "ape_spatial_steps_per_s",
+                "wilson_R9T9": "wilson_R9T9_sweeps_per_s", "qtop": "qtop_per_s"}
+    for k, p in ps.items():
+        txt, _ = p.communicate()
+        ts = [float(line.split()[3]) for line in txt.splitlines() if line.startswith("RESULT") and line.split()[1]
+              .endswith("_s")]
+        if p.returncode != 0 or not ts:
+            continue
+        t_ref = min(ts) * scale
+        e = {"cpu_ref_s_per_unit": t_ref}
+        for prec in ("fp64", "fp32"):
+            r = gpu.get(f"{prec}_{gpu_rate[k]}")
+            if r:
+                e[f"gpu_{prec}_s_per_unit"] = 1.0 / r
+                e[f"speedup_{prec}_vs_1_core"] = t_ref * r
+        out[k] = e
+    return out
+
+
 def run_reference(args, dist, dims):
     if dist.rank != 0:
         return
@@ -430,6 +463,20 @@ def run_ours(args, dist, dims):
     if not args.no_extras:
         extras["batch"] = batch_figures(dist)
         extras["graph_loop"] = graph_figures(dist)
+        # one configuration's measurement (the 48^4 flows of the thesis: 400 spatial APE steps then
+        # W(R<=9, T<=9); Q after 30 APE_all steps), one CUDA graph per configuration
+        R9 = [r for r in range(1, 10) for t in range(1, 10)]
+        T9 = [t for r in range(1, 10) for t in range(1, 10)]
+        spec = dict(q_ape=[30], alpha_q=0.5, R=R9, T=T9, ns_t=0, alpha_t=0.0, ns_s=400, alpha_s=0.5)
+        lat.measure(**spec)
+        reps = 3
+        lat.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            lat.measure(**spec)
+        extras["measurement_fp32_ms_per_configuration"] = (time.perf_counter() - t0) * 1e3 / reps
+        extras["measurement_spec"] = "Q after 30 APE_all (alpha 0.5); W(R<=9, T<=9) after 400 spatial APE (alpha 0.5)"
+        lat.measure_release()
     line["extras"] = extras
 
     # end to end through the C ABI with host buffers: upload the configuration from pinned host
@@ -458,6 +505,10 @@ def run_ours(args, dist, dims):
         res = cpu_reference_rate(dims, 1, 0, 200_000)
         line["cpu_baseline"] = {"value": res["rates"][0], "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
                                 "sample": res["sample"], "cpu_model": res["model"], "nproc": res["nproc"]}
+        if not args.no_extras:
+            ck = cpu_reference_kernels(extras, dims)
+            if ck:
+                extras["cpu_reference_kernels"] = ck
     lat.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

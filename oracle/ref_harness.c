@@ -298,6 +298,55 @@ int main(int argc, char *argv[])
         return 0;
     }
 
+    /* bench_wil <rmax> <tmax> <reps>: measureWilsonLoop (wilson.c:268-324) over the grid R <= rmax,
+     * T <= tmax on a hot start, timed per rep */
+    if (strcmp(cmd, "bench_wil") == 0) {
+        if (argc != 5) die("bench_wil <rmax> <tmax> <reps>");
+        int rmax = atoi(argv[2]), tmax = atoi(argv[3]), reps = atoi(argv[4]), nl = 0;
+        static int R[1024], T[1024];
+        static double w[1024];
+        if (rmax * tmax > 1024) die("too many loops");
+        for (int r = 1; r <= rmax; r++)
+            for (int t = 1; t <= tmax; t++) {
+                R[nl] = r;
+                T[nl++] = t;
+            }
+        measParams.mwil_mode = nl;
+        measParams.rExtents = R;
+        measParams.tExtents = T;
+        measParams.tf = tmax;
+        rlxd_init(2, 1);
+        setup(1);
+        print_dims();
+        getTime();
+        for (int rp = 0; rp < reps; rp++) {
+            double t1 = getTime();
+            measureWilsonLoop(w);
+            double t2 = getTime();
+            printf("RESULT wil_s %d %.9f %.17g\n", rp, t2 - t1, w[0]);
+            fflush(stdout);
+        }
+        return 0;
+    }
+
+    /* bench_qtop <reps>: topologicalCharge (topologicalcharge.c:164-199) on a hot start */
+    if (strcmp(cmd, "bench_qtop") == 0) {
+        if (argc != 3) die("bench_qtop <reps>");
+        int reps = atoi(argv[2]);
+        rlxd_init(2, 1);
+        setup(1);
+        print_dims();
+        getTime();
+        for (int rp = 0; rp < reps; rp++) {
+            double t1 = getTime();
+            double q = topologicalCharge();
+            double t2 = getTime();
+            printf("RESULT qtop_s %d %.9f %.17g\n", rp, t2 - t1, q);
+            fflush(stdout);
+        }
+        return 0;
+    }
+
     /* reflect <small.cfg> <out.cfg>: readConfigForThermalisation (config_IO.c:348-535) of a
      * configuration with half this build's extents, then writeConfig of the full lattice */
     if (strcmp(cmd, "reflect") == 0) {
