@@ -6,26 +6,30 @@
 
 namespace su2g {
 
-// Walk `steps` links along direction D (negative: backwards), multiplying the path product.
+// A path walker: its product and position (lexicographic index, coordinates along A and B, parity).
+template <typename R>
+struct Walker {
+    Q<R> acc;
+    int n, ca, cb, p;
+};
+
+// One step of a walker along +D or -D (D = A or B of the plane; the coordinate tracked is ca or cb).
 // Forward: acc *= U_D(y), y += D.  Backward: y -= D, acc *= U_D(y)^dag  (computeLine,
 // topologicalcharge.c:18-44).
-template <typename R, int D>
-__device__ __forceinline__ void walk(const Field<R>& U, const Geom& g, int& n, int& c, int& par, int steps, Q<R>& acc)
+template <typename R, int D, bool FWD, bool ISA>
+__device__ __forceinline__ void wstep(const Field<R>& U, const Geom& g, Walker<R>& w)
 {
-    if (steps > 0) {
-        for (int i = 0; i < steps; ++i) {
-            acc = q_mul(acc, U.ld(D, par, n));
-            if (c == g.L[D] - 1) { n -= (g.L[D] - 1) * g.S[D]; c = 0; }
-            else { n += g.S[D]; ++c; }
-            par ^= 1;
-        }
+    int& c = ISA ? w.ca : w.cb;
+    if (FWD) {
+        w.acc = q_mul(w.acc, U.ld(D, w.p, w.n));
+        if (c == g.L[D] - 1) { w.n -= (g.L[D] - 1) * g.S[D]; c = 0; }
+        else { w.n += g.S[D]; ++c; }
+        w.p ^= 1;
     } else {
-        for (int i = 0; i < -steps; ++i) {
-            if (c == 0) { n += (g.L[D] - 1) * g.S[D]; c = g.L[D] - 1; }
-            else { n -= g.S[D]; --c; }
-            par ^= 1;
-            acc = q_mul_nd(acc, U.ld(D, par, n));
-        }
+        if (c == 0) { w.n += (g.L[D] - 1) * g.S[D]; c = g.L[D] - 1; }
+        else { w.n -= g.S[D]; --c; }
+        w.p ^= 1;
+        w.acc = q_mul_nd(w.acc, U.ld(D, w.p, w.n));
     }
 }
 
@@ -33,33 +37,46 @@ __device__ __forceinline__ void walk(const Field<R>& U, const Geom& g, int& n, i
 // F = [(k1 C1 + k2 C2 + k3 C3) - h.c.]/2 with C_e = (1/4) sum of the four e x e leaves and
 // (k1, k2, k3) = (1.5, -0.15, 1/90)  (computeCloverAverages / computeCloverProducts /
 // hermitianTraceless, topologicalcharge.c:46-162).  The leaves, all starting and ending at x:
-//   +A +B -A -B,   -B +A +B -A,   +B -A -B +A,   -A -B +A +B.
+//   +A +B -A -B,   -B +A +B -A,   +B -A -B +A,   -A -B +A +B
+// (each segment e links long).  The four leaves walk in lockstep, one step each per iteration, so
+// a thread keeps four independent product chains in flight.  The clover sizes run as a loop, not
+// unrolled, which keeps the register count low enough for two CTAs per SM.
 template <typename R, int A, int B>
 __device__ __forceinline__ Q<R> clover_F(const Field<R>& U, const Geom& g, const Site& s, int par)
 {
-    const R kcoef[3] = {R(1.5), R(-0.15), R(1.0 / 90.0)};
     Q<R> F = q_zero<R>();
-#pragma unroll
+#pragma unroll 1
     for (int e = 1; e <= 3; ++e) {
-        Q<R> C = q_zero<R>();
-        int n = s.n, ca = s.c[A], cb = s.c[B], p = par;
-        Q<R> l = q_one<R>();
-        walk<R, A>(U, g, n, ca, p, e, l); walk<R, B>(U, g, n, cb, p, e, l);
-        walk<R, A>(U, g, n, ca, p, -e, l); walk<R, B>(U, g, n, cb, p, -e, l);
-        C = q_add(C, l);
-        l = q_one<R>();
-        walk<R, B>(U, g, n, cb, p, -e, l); walk<R, A>(U, g, n, ca, p, e, l);
-        walk<R, B>(U, g, n, cb, p, e, l); walk<R, A>(U, g, n, ca, p, -e, l);
-        C = q_add(C, l);
-        l = q_one<R>();
-        walk<R, B>(U, g, n, cb, p, e, l); walk<R, A>(U, g, n, ca, p, -e, l);
-        walk<R, B>(U, g, n, cb, p, -e, l); walk<R, A>(U, g, n, ca, p, e, l);
-        C = q_add(C, l);
-        l = q_one<R>();
-        walk<R, A>(U, g, n, ca, p, -e, l); walk<R, B>(U, g, n, cb, p, -e, l);
-        walk<R, A>(U, g, n, ca, p, e, l); walk<R, B>(U, g, n, cb, p, e, l);
-        C = q_add(C, l);
-        F = q_axpy(kcoef[e - 1] * R(0.25), C, F);
+        const R kcoef = e == 1 ? R(1.5) : (e == 2 ? R(-0.15) : R(1.0 / 90.0));
+        Walker<R> w[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) w[i] = Walker<R>{q_one<R>(), s.n, s.c[A], s.c[B], par};
+        for (int i = 0; i < e; ++i) {   // segment 1: +A, -B, +B, -A
+            wstep<R, A, true, true>(U, g, w[0]);
+            wstep<R, B, false, false>(U, g, w[1]);
+            wstep<R, B, true, false>(U, g, w[2]);
+            wstep<R, A, false, true>(U, g, w[3]);
+        }
+        for (int i = 0; i < e; ++i) {   // segment 2: +B, +A, -A, -B
+            wstep<R, B, true, false>(U, g, w[0]);
+            wstep<R, A, true, true>(U, g, w[1]);
+            wstep<R, A, false, true>(U, g, w[2]);
+            wstep<R, B, false, false>(U, g, w[3]);
+        }
+        for (int i = 0; i < e; ++i) {   // segment 3: -A, +B, -B, +A
+            wstep<R, A, false, true>(U, g, w[0]);
+            wstep<R, B, true, false>(U, g, w[1]);
+            wstep<R, B, false, false>(U, g, w[2]);
+            wstep<R, A, true, true>(U, g, w[3]);
+        }
+        for (int i = 0; i < e; ++i) {   // segment 4: -B, -A, +A, +B
+            wstep<R, B, false, false>(U, g, w[0]);
+            wstep<R, A, false, true>(U, g, w[1]);
+            wstep<R, A, true, true>(U, g, w[2]);
+            wstep<R, B, true, false>(U, g, w[3]);
+        }
+        const Q<R> C = q_add(q_add(w[0].acc, w[1].acc), q_add(w[2].acc, w[3].acc));
+        F = q_axpy(kcoef * R(0.25), C, F);
     }
     F.c0 = R(0);   // (F - F^dag)/2 keeps the su(2) part
     return F;

@@ -244,8 +244,9 @@ __device__ __forceinline__ double qtop_density(const Field<R>& U, const Geom& g,
 }
 
 // One site per thread; CTA partials of q and |q| at partials[b] and partials[gridDim.x + b].
+// FP32: two resident CTAs per SM (at most 128 registers a thread); FP64 needs more registers.
 template <typename R>
-__global__ void __launch_bounds__(kBlock) k_qtop(Field<R> U, Geom g, DD* __restrict__ partials)
+__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 2 : 1) k_qtop(Field<R> U, Geom g, DD* __restrict__ partials)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double d = 0.0;
