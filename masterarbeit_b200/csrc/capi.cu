@@ -360,6 +360,7 @@ extern "C" int su2g_create(const su2g_params* p, su2g_lattice** out)
         rc = check_cuda(h, e, "allocating status word");
     if (!rc) rc = check_cuda(h, cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream), "clearing status");
     if (!rc) rc = ensure_partials(h, 2);
+    if (!rc) wilson_prepare(h);
     if (!rc) rc = check_cuda(h, cudaEventCreate(&h->ev_begin), "creating events");
     if (!rc) rc = check_cuda(h, cudaEventCreate(&h->ev_end), "creating events");
     if (!rc) rc = su2g_start(h, p->start, p->seed);

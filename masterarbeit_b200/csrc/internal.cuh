@@ -195,6 +195,8 @@ void release_run_graph(su2g_lattice* h);
 // index of pair i.  Fails (nothing enqueued) if the pairs need more than `max_slots` slots.
 int wilson_enqueue(su2g_lattice* h, void* const dirs[4], const int32_t* R, const int32_t* T, int n, int out_off,
                    int max_slots, int* slot);
+// Raise the dynamic shared memory limit of the Wilson loop kernels (once per handle, at creation).
+void wilson_prepare(su2g_lattice* h);
 // Check R, T >= 1 and T <= L_t - 1 (measureWilsonLoop, wilson.c:290-291).
 int wilson_check(su2g_lattice* h, const int32_t* R, const int32_t* T, int n, const char* who);
 // Enqueue the plaquette of the current field into d_out[out_off].

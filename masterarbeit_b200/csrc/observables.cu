@@ -70,9 +70,17 @@ __host__ __device__ constexpr bool ape_staple(int mode, int mu, int nu)
 // The middle product P = U_mu(x+nu) U_nu(x+mu)^dag of the forward staple of mu in plane nu is
 // also the dagger of the middle product of the forward staple of nu in plane mu, so each plane's
 // P is formed once.  Reads `in`, writes only the updated directions of `out`.
-// Two resident CTAs per SM: measured faster than 3 or 4 on B200 (a CTA's neighbours need L1 room).
+// Resident CTAs per SM, measured at 48^4 on B200 against 2, 3 and 4: APE_all 2 (more thrash L1;
+// 255 us FP32), spatial 4 in FP32 (136 us against 164 us with 2) but 2 in FP64 (more spill),
+// temporal 4 (98 us FP32, 211 us FP64).
 template <typename R, int MODE>
-__global__ void __launch_bounds__(kBlock, 2) k_ape(Field<R> in, Field<R> out, Geom g, R alpha)
+constexpr int ape_min_blocks()
+{
+    return MODE == SU2G_APE_ALL ? 2 : (sizeof(R) == 4 || MODE == SU2G_APE_TEMPORAL ? 4 : 2);
+}
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(kBlock, ape_min_blocks<R, MODE>()) k_ape(Field<R> in, Field<R> out, Geom g, R alpha)
 {
     // one site per thread; CTAs dispatched in order, alternating parity over the same h run
     Site s;
@@ -230,6 +238,113 @@ __global__ void __launch_bounds__(kBlock) k_wilson(Field<R> U, Geom g, int r0, i
     }
 }
 
+// Column form of the same sums.  A CTA owns `sw` consecutive spatial sites s (the lexicographic
+// index within a time slice) in every time slice; thread t * sw + j takes site t S0 + s0 + j.  Per
+// spatial direction K each thread stores its spatial lines S_{r0+r}(x) in shared memory, so the
+// line at x + T t that the loop needs for every T is the one the thread of slice t + T stored:
+// it is read, not rebuilt, which removes the longest product chain of the per-site form.
+constexpr int kWilsonColMaxThreads = 512;
+
+template <typename R, int K, int RC>
+__device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g, Q<R>* __restrict__ line,
+                                               DD* __restrict__ wacc, int sw, int t, int j, int s, bool valid, int r0,
+                                               int tlo, int thi)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nT = thi - tlo + 1;
+    int par;
+    const int n = t * g.S[0] + s;
+    const Site st = site_lex(g, n, par);
+    Q<R>* own = line + (size_t)threadIdx.x * RC;
+    int xr[RC];   // lexicographic index of x + (r0 + r) k
+    Q<R> S = q_one<R>();
+    for (int jj = 0; jj < r0 - 1; ++jj) S = q_mul(S, U.ld(K, par ^ (jj & 1), n + shift_k<K>(g, st.c[K], jj)));
+#pragma unroll
+    for (int r = 0; r < RC; ++r) {
+        const int jj = r0 - 1 + r;
+        S = q_mul(S, U.ld(K, par ^ (jj & 1), n + shift_k<K>(g, st.c[K], jj)));
+        own[r] = S;
+        xr[r] = n + shift_k<K>(g, st.c[K], jj + 1);
+    }
+    __syncthreads();
+    Q<R> TX = q_one<R>(), TR[RC];
+#pragma unroll
+    for (int r = 0; r < RC; ++r) TR[r] = q_one<R>();
+    for (int T = 1; T <= thi; ++T) {
+        const int tprev = shift_t(g, st.c[0], T - 1);
+        const int pprev = par ^ ((T - 1) & 1);
+        TX = q_mul(TX, U.ld(0, pprev, n + tprev));
+#pragma unroll
+        for (int r = 0; r < RC; ++r) TR[r] = q_mul(TR[r], U.ld(0, pprev ^ ((r0 + r) & 1), xr[r] + tprev));
+        if (T < tlo) continue;
+        int tt = t + T;
+        if (tt >= g.L[0]) tt -= g.L[0];
+        const Q<R>* other = line + (size_t)(tt * sw + j) * RC;   // S_{r0+r}(x + T t)
+#pragma unroll
+        for (int r = 0; r < RC; ++r) {
+            double w = valid ? (double)q_dot(q_mul(TX, other[r]), q_mul(own[r], TR[r])) : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+            if (lane == 0) {
+                DD* slot = wacc + ((size_t)warp * RC + r) * nT + (T - tlo);
+                *slot = dd_add(*slot, w);
+            }
+        }
+    }
+    __syncthreads();   // `line` is overwritten next
+}
+
+template <typename R, int RC>
+__global__ void __launch_bounds__(kWilsonColMaxThreads, 1) k_wilson_col(Field<R> U, Geom g, int sw, int r0, int tlo,
+                                                                        int thi, DD* __restrict__ partials)
+{
+    extern __shared__ __align__(16) unsigned char wsm[];
+    Q<R>* line = (Q<R>*)wsm;
+    const int nwarps = blockDim.x >> 5, nT = thi - tlo + 1;
+    DD* wacc = (DD*)(wsm + (size_t)blockDim.x * RC * sizeof(Q<R>));
+    for (int i = threadIdx.x; i < nwarps * RC * nT; i += blockDim.x) wacc[i] = DD{0.0, 0.0};
+    __syncthreads();
+    const int t = threadIdx.x / sw, j = threadIdx.x % sw;
+    const int stot = g.S[0], ntiles = (stot + sw - 1) / sw;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int s_req = tile * sw + j;
+        const bool valid = s_req < stot;
+        const int s = valid ? s_req : stot - 1;   // threads past the end read a valid site and add 0
+        wilson_col_dir<R, 1, RC>(U, g, line, wacc, sw, t, j, s, valid, r0, tlo, thi);
+        wilson_col_dir<R, 2, RC>(U, g, line, wacc, sw, t, j, s, valid, r0, tlo, thi);
+        wilson_col_dir<R, 3, RC>(U, g, line, wacc, sw, t, j, s, valid, r0, tlo, thi);
+    }
+    // fixed-order sum over warps; slot r * kWilsonTChunk + (T - tlo) as in k_wilson
+    for (int i = threadIdx.x; i < RC * nT; i += blockDim.x) {
+        const int r = i / nT, ti = i % nT;
+        DD v = {0.0, 0.0};
+        for (int w = 0; w < nwarps; ++w) v = dd_add(v, wacc[((size_t)w * RC + r) * nT + ti]);
+        partials[(size_t)(r * kWilsonTChunk + ti) * kMaxPartials + blockIdx.x] = v;
+    }
+}
+
+// Spatial sites per CTA for the column kernel: the smallest sw with L_t sw a multiple of 32 and at
+// least 256 threads; 0 if that exceeds kWilsonColMaxThreads (the per-site kernel then runs).
+int wilson_col_width(const Geom& g)
+{
+    int a = g.L[0], b = 32;
+    while (b) {
+        const int r = a % b;
+        a = b;
+        b = r;
+    }
+    const int m = 32 / a;
+    if (g.L[0] * m > kWilsonColMaxThreads) return 0;
+    int sw = m;
+    while (g.L[0] * (sw + m) <= kWilsonColMaxThreads && g.L[0] * sw < 256) sw += m;
+    return sw;
+}
+
+template <typename R, int RC>
+size_t wilson_col_smem(int threads, int nT)
+{
+    return (size_t)threads * RC * sizeof(Q<R>) + (size_t)(threads / 32) * RC * nT * sizeof(DD);
+}
+
 // --------------------------------------------------- topological charge ---
 
 // q(x) = 8 [tr F01 F23 + tr F02 F31 + tr F03 F12], tr = 2 c0 (topologicalcharge.c:175-178)
@@ -286,21 +401,46 @@ void launch_ape(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4]
     else k_ape<R, SU2G_APE_TEMPORAL><<<grid, kBlock, 0, h->stream>>>(in, out, h->g, alpha);
 }
 
+// Launch one chunk of loops; returns the number of CTAs (= partials per slot), 0 on a launch error.
 template <typename R, int RC>
-void launch_wilson_t(su2g_lattice* h, void* const dirs[4], int r0, int tlo, int thi, int grid)
+int launch_wilson_t(su2g_lattice* h, void* const dirs[4], int r0, int tlo, int thi)
 {
-    k_wilson<R, RC><<<grid, kBlock, 0, h->stream>>>(make_field<R>(dirs, h->g.Vh), h->g, r0, tlo, thi, h->partials);
+    const Field<R> U = make_field<R>(dirs, h->g.Vh);
+    const int sw = wilson_col_width(h->g);
+    if (sw > 0) {
+        const int threads = sw * h->g.L[0];
+        const size_t smem = wilson_col_smem<R, RC>(threads, thi - tlo + 1);
+        int per_sm = 0;
+        if (smem <= (size_t)h->max_smem &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wilson_col<R, RC>, threads, smem) == cudaSuccess &&
+            per_sm > 0) {
+            const int ntiles = (h->g.S[0] + sw - 1) / sw;
+            const int grid = std::max(1, std::min(std::min(ntiles, h->num_sms * per_sm), kMaxPartials));
+            k_wilson_col<R, RC><<<grid, threads, smem, h->stream>>>(U, h->g, sw, r0, tlo, thi, h->partials);
+            return grid;
+        }
+        cudaGetLastError();
+    }
+    const int grid = resident_grid(h, (const void*)k_wilson<R, RC>, h->g.V);
+    k_wilson<R, RC><<<grid, kBlock, 0, h->stream>>>(U, h->g, r0, tlo, thi, h->partials);
+    return grid;
 }
 
 template <typename R>
-void launch_wilson(su2g_lattice* h, void* const dirs[4], int rc, int r0, int tlo, int thi, int grid)
+int launch_wilson(su2g_lattice* h, void* const dirs[4], int rc, int r0, int tlo, int thi)
 {
     switch (rc) {
-        case 1: launch_wilson_t<R, 1>(h, dirs, r0, tlo, thi, grid); break;
-        case 2: launch_wilson_t<R, 2>(h, dirs, r0, tlo, thi, grid); break;
-        case 4: launch_wilson_t<R, 4>(h, dirs, r0, tlo, thi, grid); break;
-        default: launch_wilson_t<R, 8>(h, dirs, r0, tlo, thi, grid); break;
+        case 1: return launch_wilson_t<R, 1>(h, dirs, r0, tlo, thi);
+        case 2: return launch_wilson_t<R, 2>(h, dirs, r0, tlo, thi);
+        case 4: return launch_wilson_t<R, 4>(h, dirs, r0, tlo, thi);
+        default: return launch_wilson_t<R, 8>(h, dirs, r0, tlo, thi);
     }
+}
+
+template <typename R, int RC>
+void wilson_smem_attr(int bytes)
+{
+    cudaFuncSetAttribute(k_wilson_col<R, RC>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 }  // namespace
@@ -383,6 +523,20 @@ extern "C" int su2g_ape(su2g_lattice* h, int32_t ns, double alpha, int32_t mode)
     return ape_enqueue(h, ns, alpha, mode);
 }
 
+void su2g::wilson_prepare(su2g_lattice* h)
+{
+    // the column kernel's dynamic shared memory can exceed the 48 KB default; allowed once per handle
+    wilson_smem_attr<float, 1>(h->max_smem);
+    wilson_smem_attr<float, 2>(h->max_smem);
+    wilson_smem_attr<float, 4>(h->max_smem);
+    wilson_smem_attr<float, 8>(h->max_smem);
+    wilson_smem_attr<double, 1>(h->max_smem);
+    wilson_smem_attr<double, 2>(h->max_smem);
+    wilson_smem_attr<double, 4>(h->max_smem);
+    wilson_smem_attr<double, 8>(h->max_smem);
+    cudaGetLastError();
+}
+
 int su2g::wilson_check(su2g_lattice* h, const int32_t* R, const int32_t* T, int n, const char* who)
 {
     int tmax = 0;
@@ -413,8 +567,12 @@ int su2g::wilson_enqueue(su2g_lattice* h, void* const dirs[4], const int32_t* R,
     std::vector<Chunk> plan;
     std::vector<int> slot_rt((size_t)rmax * tmax, -1);
     int used = 0;
+    // the column kernel reads the lines at x + T t instead of rebuilding them, so narrow R chunks
+    // cost it little, and 4 keeps it at two CTAs per SM; the per-site kernel prefers 8
+    const int rc_max = wilson_col_width(h->g) > 0 ? 4 : 8;
     for (int r0 = 1; r0 <= rmax;) {
-        const int left = rmax - r0 + 1, rc_n = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
+        const int left = rmax - r0 + 1;
+        const int rc_n = left >= 8 && rc_max >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
         for (int tlo = 1; tlo <= tmax; tlo += kWilsonTChunk) {
             const int thi = std::min(tmax, tlo + kWilsonTChunk - 1);
             bool any = false;
@@ -433,12 +591,10 @@ int su2g::wilson_enqueue(su2g_lattice* h, void* const dirs[4], const int32_t* R,
         return set_error(h, SU2G_EINVAL, "Wilson loops: %d result slots needed, %d available", used, max_slots);
     int rc = ensure_partials(h, 8 * kWilsonTChunk);
     if (rc) return rc;
-    const int grid = h->prec == SU2G_FP32 ? resident_grid(h, (const void*)k_wilson<float, 8>, h->g.V)
-                                          : resident_grid(h, (const void*)k_wilson<double, 8>, h->g.V);
     for (const Chunk& c : plan) {
         launch_begin(h, SU2G_K_WILSON);
-        if (h->prec == SU2G_FP32) launch_wilson<float>(h, dirs, c.rc_n, c.r0, c.tlo, c.thi, grid);
-        else launch_wilson<double>(h, dirs, c.rc_n, c.r0, c.tlo, c.thi, grid);
+        const int grid = h->prec == SU2G_FP32 ? launch_wilson<float>(h, dirs, c.rc_n, c.r0, c.tlo, c.thi)
+                                              : launch_wilson<double>(h, dirs, c.rc_n, c.r0, c.tlo, c.thi);
         if ((rc = launch_end(h, SU2G_K_WILSON, "Wilson loop kernel"))) return rc;
         // W = sum_x,k c0 / (3 V)  (wilson.c:322: sum of Re tr / (3 V 2))
         if ((rc = finalize(h, grid, c.rc_n * kWilsonTChunk, 1.0 / (3.0 * (double)h->g.V), c.base))) return rc;

@@ -237,3 +237,20 @@ def test_observables_vs_oracle_random(dims):
     assert abs(q - qo) <= 1e-12 * sabs
     L.ape(2, 0.5, "spatial")
     assert np.max(np.abs(L.download() - O.ape(dims, U, 2, 0.5, "spatial"))) <= 1e-13
+
+
+@pytest.mark.parametrize("dims", [(34, 4, 4, 4), (10, 6, 4, 6), (12, 4, 6, 2), (48, 2, 2, 2)])
+def test_wilson_kernels_against_oracle(dims):
+    """The column Wilson-loop kernel (time extents whose CTA fits: 10, 12, 48, with ragged last
+    tiles) and the per-site kernel (L_t = 34, whose column CTA would exceed the thread limit),
+    against the oracle, R up to 9 (chunks of 4/2/1 and 8/1) and T up to 31."""
+    L = Lattice(dims, precision="fp64", seed=31, start="haar")
+    U = L.download()
+    rmax, tmax = 9, min(dims[0] - 1, 31)
+    R = [r for r in range(1, rmax + 1) for t in range(1, tmax + 1)]
+    T = [t for r in range(1, rmax + 1) for t in range(1, tmax + 1)]
+    ref = O.wilson(dims, U, R, T)
+    assert np.max(np.abs(L.wilson(R, T) - ref)) <= 1e-13
+    L32 = Lattice(dims, precision="fp32")
+    L32.upload(U)
+    assert np.max(np.abs(L32.wilson(R, T) - ref)) <= 2e-6
