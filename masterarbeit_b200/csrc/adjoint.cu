@@ -86,7 +86,6 @@ __global__ void __launch_bounds__(kBlock) k_qgrad_fbar(Field<R> U, Geom g, R* __
     if (i >= g.V) return;
     int par;
     const Site s = site_lex(g, i, par);
-    const int h = i >> 1;
     const size_t V = (size_t)g.V, n = (size_t)s.n;
     Q<R> f0 = clover_F<R, 0, 1>(U, g, s, par), f1 = clover_F<R, 2, 3>(U, g, s, par);
     stq(fbar, 0 * V + n, q_scale(f1, -scale));
@@ -185,7 +184,6 @@ __global__ void __launch_bounds__(kBlock) k_qgrad_scatter(Field<R> U, Field<R> G
     if (i >= g.V) return;
     int par;
     const Site s = site_lex(g, i, par);
-    const int h = i >> 1;
     const Q<R> Fbar = ldq(fbar, (size_t)PLANE * g.V + (size_t)s.n);
     clover_adjoint_e<R, A, B, 1>(U, G, g, s, par, Fbar);
     clover_adjoint_e<R, A, B, 2>(U, G, g, s, par, Fbar);

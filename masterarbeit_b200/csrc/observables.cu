@@ -215,7 +215,6 @@ __global__ void __launch_bounds__(kBlock) k_wilson(Field<R> U, Geom g, int r0, i
         const int ii = valid ? i : i0;   // inactive lanes recompute a valid site and contribute 0
         int par;
         const Site s = site_lex(g, ii, par);
-        const int h = ii >> 1;
         DD* acc = &wacc[warp][0];
         // Lanes past the end recompute a valid site with an empty record window (tlo > thi), so
         // that every lane takes part in the warp shuffles.
@@ -281,12 +280,14 @@ __device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g,
         const Q<R>* other = line + (size_t)(tt * sw + j) * RC;   // S_{r0+r}(x + T t)
 #pragma unroll
         for (int r = 0; r < RC; ++r) {
-            double w = valid ? (double)q_dot(q_mul(TX, other[r]), q_mul(own[r], TR[r])) : 0.0;
+            // the 32 lanes' terms are summed in the link precision (FP32: one shuffle per step; its
+            // rounding, ~1e-7 of a warp sum, is far below the FP32 links' own), then compensated FP64
+            R w = valid ? q_dot(q_mul(TX, other[r]), q_mul(own[r], TR[r])) : R(0);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
             if (lane == 0) {
                 DD* slot = wacc + ((size_t)warp * RC + r) * nT + (T - tlo);
-                *slot = dd_add(*slot, w);
+                *slot = dd_add(*slot, (double)w);
             }
         }
     }
@@ -368,7 +369,6 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 2 : 1) k_qtop(Field<R
     if (i < g.V) {
         int par;
         const Site s = site_lex(g, i, par);
-        const int h = i >> 1;
         d = qtop_density<R>(U, g, s, par);
     }
     DD acc = dd_block_sum<kBlock>(DD{d, 0.0});
