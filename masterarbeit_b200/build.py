@@ -14,8 +14,7 @@ REPO = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libsu2g.so")
-DRIVER_SRC = os.path.join(PKG, "driver", "su2meas.cpp")
-DRIVER = os.path.join(LIBDIR, "su2meas")
+DRIVERS = ("su2meas", "su2qcd")   # native drivers, driver/<name>.cpp -> _lib/<name>
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
@@ -65,18 +64,19 @@ def build(force=False, verbose=False, extra=()):
 
 
 def build_driver(force=False):
-    """The native measurement driver (host C++ over the C ABI), next to the library."""
-    if not force and os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(
-            os.path.getmtime(DRIVER_SRC), os.path.getmtime(LIB)):
-        return DRIVER
+    """The native drivers (host C++ over the C ABI), next to the library."""
     cxx = shutil.which("g++") or "g++"
-    cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(REPO, "include"), DRIVER_SRC, "-L", LIBDIR,
-           "-lsu2g", "-Wl,-rpath,$ORIGIN", "-o", DRIVER + ".tmp"]
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        raise RuntimeError("building su2meas failed:\n" + res.stdout + res.stderr)
-    os.replace(DRIVER + ".tmp", DRIVER)
-    return DRIVER
+    for name in DRIVERS:
+        src, out = os.path.join(PKG, "driver", name + ".cpp"), os.path.join(LIBDIR, name)
+        if not force and os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(src),
+                                                                               os.path.getmtime(LIB)):
+            continue
+        cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(REPO, "include"), src, "-L", LIBDIR, "-lsu2g",
+               "-Wl,-rpath,$ORIGIN", "-o", out + ".tmp"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"building {name} failed:\n" + res.stdout + res.stderr)
+        os.replace(out + ".tmp", out)
 
 
 if __name__ == "__main__":

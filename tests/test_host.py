@@ -127,3 +127,22 @@ def test_su2meas_argument_and_input_errors(tmp_path):
                    "mwil 0 6\ntSmear 0 0.5\nrSmear 0 0.5\nmcorrs 1\n")
     r = subprocess.run([driver, "-i", str(inp), "-d", "4x4x4x4"], capture_output=True, text=True)
     assert r.returncode == 1 and "two-point functions" in r.stderr
+
+
+def test_su2qcd_input_errors(tmp_path):
+    """The native qcd driver refuses incomplete input files and existing logs before it touches a GPU."""
+    import subprocess
+
+    driver = os.path.join(O.REPO, "masterarbeit_b200", "_lib", "su2qcd")
+    if not os.path.exists(driver):
+        pytest.skip("su2qcd not built")
+    assert subprocess.run([driver], capture_output=True).returncode == 2
+    inp = tmp_path / "qcd.in"
+    inp.write_text("outFileId 1\noutputDir %s\nstart 0\nbeta 3.09\n" % tmp_path)
+    r = subprocess.run([driver, "-i", str(inp), "-d", "4x4x4x4"], capture_output=True, text=True)
+    assert r.returncode == 1 and "missing field" in r.stderr
+    inp.write_text("outFileId 1\noutputDir %s\nstart 0\nbeta 3.09\nepsilon 0.1\nnconf 2\nntherm 0\nndecorr 1\n"
+                   "writeConfFreq 0\nseed 1\n" % tmp_path)
+    (tmp_path / "4x4x4x4_SU2_b3.090000_id1.log").write_text("old run\n")
+    r = subprocess.run([driver, "-i", str(inp), "-d", "4x4x4x4"], capture_output=True, text=True)
+    assert r.returncode == 1 and "overwrite" in r.stderr
