@@ -448,14 +448,20 @@ def run_ours(args, dist, dims):
                 extras[f"{prec}_ape_{mode}_frac_of_peak"] = extras[f"{prec}_ape_{mode}_gbs"] / peak
             R = [r for r in range(1, 10) for t in range(1, 10)]
             T = [t for r in range(1, 10) for t in range(1, 10)]
+            # ALU-bound rows: algorithmic flops (line method: 765 quaternion products per site for
+            # R, T <= 9; clover charge: 576 products per site; 28 flop a product) against the nominal
+            # FP32 / FP64 rate of 148 SMs x 128 / 64 lanes x 2 flop at the SM clock sampled above
+            f_mhz = (clk or {}).get("sm_mhz") or 1965.0
+            alu_peak = 148 * (128 if prec == "fp32" else 64) * 2 * f_mhz * 1e6
+            extras[f"{prec}_alu_peak_tflops_nominal"] = alu_peak / 1e12
             L.wilson([1], [1])
-            t0 = time.perf_counter()
-            L.wilson(R, T)
-            extras[f"{prec}_wilson_R9T9_sweeps_per_s"] = 1.0 / (time.perf_counter() - t0)
+            ms_w = time_steps(L, 1, lambda: L.wilson(R, T))
+            extras[f"{prec}_wilson_R9T9_sweeps_per_s"] = 1e3 / ms_w
+            extras[f"{prec}_wilson_R9T9_frac_of_alu_peak"] = vol * 765 * 28 / (ms_w / 1e3) / alu_peak
             L.qtop()
-            t0 = time.perf_counter()
-            L.qtop()
-            extras[f"{prec}_qtop_per_s"] = 1.0 / (time.perf_counter() - t0)
+            ms_q = time_steps(L, 1, L.qtop)
+            extras[f"{prec}_qtop_per_s"] = 1e3 / ms_q
+            extras[f"{prec}_qtop_frac_of_alu_peak"] = vol * 576 * 28 / (ms_q / 1e3) / alu_peak
             if prec == "fp64":
                 L.close()
         extras["fp32_over_fp64_link_updates"] = value / dist.world / extras["fp64_link_updates_per_s"]

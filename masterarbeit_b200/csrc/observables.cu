@@ -73,14 +73,22 @@ __host__ __device__ constexpr bool ape_staple(int mode, int mu, int nu)
 // Resident CTAs per SM, measured at 48^4 on B200 against 2, 3 and 4: APE_all 2 (more thrash L1;
 // 255 us FP32), spatial 4 in FP32 (136 us against 164 us with 2) but 2 in FP64 (more spill),
 // temporal 4 (98 us FP32, 211 us FP64).
+// FP32 APE_all runs 128-thread CTAs, five per SM (at most 102 registers): 239 us against 254 us with
+// two 256-thread CTAs (the scheduler holding 4 warps of a 128-register kernel); FP64 spills there.
 template <typename R, int MODE>
 constexpr int ape_min_blocks()
 {
-    return MODE == SU2G_APE_ALL ? 2 : (sizeof(R) == 4 || MODE == SU2G_APE_TEMPORAL ? 4 : 2);
+    return MODE == SU2G_APE_ALL ? (sizeof(R) == 4 ? 5 : 2) : (sizeof(R) == 4 || MODE == SU2G_APE_TEMPORAL ? 4 : 2);
+}
+template <typename R, int MODE>
+constexpr int ape_block()
+{
+    return MODE == SU2G_APE_ALL && sizeof(R) == 4 ? 128 : kBlock;
 }
 
 template <typename R, int MODE>
-__global__ void __launch_bounds__(kBlock, ape_min_blocks<R, MODE>()) k_ape(Field<R> in, Field<R> out, Geom g, R alpha)
+__global__ void __launch_bounds__(ape_block<R, MODE>(), ape_min_blocks<R, MODE>()) k_ape(Field<R> in, Field<R> out,
+                                                                                        Geom g, R alpha)
 {
     // one site per thread; CTAs dispatched in order, alternating parity over the same h run
     Site s;
@@ -396,13 +404,21 @@ int ensure_alt(su2g_lattice* h)
     return SU2G_OK;
 }
 
+template <typename R, int MODE>
+void launch_ape_t(su2g_lattice* h, const Field<R>& in, const Field<R>& out, R alpha)
+{
+    constexpr int block = ape_block<R, MODE>();
+    const int grid = 2 * (int)((h->g.Vh + block - 1) / block);   // CTA pairs over the same h run
+    k_ape<R, MODE><<<grid, block, 0, h->stream>>>(in, out, h->g, alpha);
+}
+
 template <typename R>
-void launch_ape(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], int mode, R alpha, int grid)
+void launch_ape(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], int mode, R alpha)
 {
     Field<R> in = make_field<R>(in_dirs, h->g.Vh), out = make_field<R>(out_dirs, h->g.Vh);
-    if (mode == SU2G_APE_ALL) k_ape<R, SU2G_APE_ALL><<<grid, kBlock, 0, h->stream>>>(in, out, h->g, alpha);
-    else if (mode == SU2G_APE_SPATIAL) k_ape<R, SU2G_APE_SPATIAL><<<grid, kBlock, 0, h->stream>>>(in, out, h->g, alpha);
-    else k_ape<R, SU2G_APE_TEMPORAL><<<grid, kBlock, 0, h->stream>>>(in, out, h->g, alpha);
+    if (mode == SU2G_APE_ALL) launch_ape_t<R, SU2G_APE_ALL>(h, in, out, alpha);
+    else if (mode == SU2G_APE_SPATIAL) launch_ape_t<R, SU2G_APE_SPATIAL>(h, in, out, alpha);
+    else launch_ape_t<R, SU2G_APE_TEMPORAL>(h, in, out, alpha);
 }
 
 // Launch one chunk of loops; returns the number of CTAs (= partials per slot), 0 on a launch error.
@@ -488,10 +504,9 @@ int su2g::ape_step(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs
         const int yb = ape_tma_rows(h->g, h->max_smem);
         if (yb > 0) return ape_tma_launch(h, in_dirs, out_dirs, alpha, yb);
     }
-    const int grid = 2 * (int)((h->g.Vh + kBlock - 1) / kBlock);
     launch_begin(h, SU2G_K_APE);
-    if (h->prec == SU2G_FP32) launch_ape<float>(h, in_dirs, out_dirs, mode, (float)alpha, grid);
-    else launch_ape<double>(h, in_dirs, out_dirs, mode, alpha, grid);
+    if (h->prec == SU2G_FP32) launch_ape<float>(h, in_dirs, out_dirs, mode, (float)alpha);
+    else launch_ape<double>(h, in_dirs, out_dirs, mode, alpha);
     return launch_end(h, SU2G_K_APE, "APE kernel");
 }
 
