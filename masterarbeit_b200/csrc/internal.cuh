@@ -58,6 +58,25 @@ __device__ __forceinline__ DD dd_warp_sum(DD v)
     return v;
 }
 
+// Block-wide sum of one double per thread: plain FP64 within each warp (32 terms, relative error
+// <= 32 ulp of the warp's partial, far below the compensated sum across warps and CTAs that
+// follows), then compensated across the warps.  Result valid in thread 0; fixed order.
+template <int NT>
+__device__ __forceinline__ DD dd_block_sum_d(double x)
+{
+    __shared__ double warp_part[NT / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) warp_part[warp] = x;
+    __syncthreads();
+    DD v = {0.0, 0.0};
+    if (threadIdx.x == 0)
+        for (int w = 0; w < NT / 32; ++w) v = dd_add(v, warp_part[w]);
+    __syncthreads();
+    return v;
+}
+
 // Block-wide compensated sum; the result is valid in thread 0.  Fixed order -> deterministic.
 template <int NT>
 __device__ __forceinline__ DD dd_block_sum(DD v)
