@@ -49,7 +49,9 @@ def parse():
 
 
 class Dist:
-    """Rank plumbing: torch.distributed over NCCL when launched by torchrun, nothing otherwise."""
+    """Rank plumbing when launched by torchrun: torch.distributed over NCCL on GPUs (gloo where no GPU
+    is visible, e.g. the CPU tests of the multi-rank path); nothing for a single process.  The ranks
+    run independent replicas and exchange only timings."""
 
     def __init__(self):
         self.rank = int(os.environ.get("RANK", "0"))
@@ -60,28 +62,32 @@ class Dist:
             import datetime
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.gpu = torch.cuda.is_available()
+            if self.gpu:
+                torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl" if self.gpu else "gloo", timeout=datetime.timedelta(seconds=300))
             self.torch = torch
             self.dist = dist
 
     def barrier(self):
         if self.torch:
-            self.dist.barrier(device_ids=[self.local])
+            if self.gpu:
+                self.dist.barrier(device_ids=[self.local])
+            else:
+                self.dist.barrier()
+
+    def _reduce(self, x, op):
+        if not self.torch:
+            return x
+        t = self.torch.tensor([float(x)], device="cuda" if self.gpu else "cpu", dtype=self.torch.float64)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
 
     def max(self, x):
-        if not self.torch:
-            return x
-        t = self.torch.tensor([float(x)], device="cuda", dtype=self.torch.float64)
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
+        return self._reduce(x, self.dist.ReduceOp.MAX) if self.torch else x
 
     def sum(self, x):
-        if not self.torch:
-            return x
-        t = self.torch.tensor([float(x)], device="cuda", dtype=self.torch.float64)
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
-        return float(t.item())
+        return self._reduce(x, self.dist.ReduceOp.SUM) if self.torch else x
 
     def close(self):
         if self.torch:
@@ -253,6 +259,8 @@ def cpu_reference_kernels(gpu, dims, ref_dims=(24, 24, 24, 24)):
 
 
 def run_reference(args, dist, dims):
+    # under torchrun rank 0 alone times the reference on the host's cores; the others do nothing
+    dist.barrier()
     if dist.rank != 0:
         return
     K, W = args.steps, args.warmup
