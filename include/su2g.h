@@ -292,6 +292,14 @@ int su2g_set_kernel_variant(su2g_lattice *h, int32_t kernel_class, int32_t varia
 int su2g_kernel_variant(const su2g_lattice *h, int32_t kernel_class, int32_t *active);
 int su2g_profile_read(su2g_lattice *h, int32_t kernel_class, int64_t *launches, double *ms);
 
+/* ---- failure detection without a GPU fault (no counterpart in the reference).  Device-side
+ * failures (a heatbath link past the Kennedy-Pendleton trial bound, a bulk copy whose wait ran out)
+ * set bits of the handle's status word; the next synchronising call returns SU2G_EDEVICE with the
+ * reason and clears the word, and the handle stays usable.  This diagnostic runs one CTA that arms
+ * an mbarrier for a bulk copy that is never issued and waits with the library's bounded wait (at
+ * most poll_limit polls, 1 ... 2^22): it returns SU2G_EDEVICE with the timeout message. */
+int su2g_selftest_bounded_wait(su2g_lattice *h, uint32_t poll_limit);
+
 #ifdef __cplusplus
 }
 #endif

@@ -19,6 +19,7 @@
 #include <cstdint>
 
 #include "internal.cuh"
+#include "mbarrier.cuh"
 
 using namespace su2g;
 
@@ -26,34 +27,6 @@ namespace {
 
 constexpr int kSlots = 10;                 // 4 centre-column slots, 3 for x+1, 3 for x-1
 constexpr uint32_t kWaitLimit = 1u << 22;  // bounded mbarrier polling
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t phase)
-{
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(bar), "r"(phase)
-        : "memory");
-    return done != 0;
-}
 
 __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
 {
@@ -147,9 +120,7 @@ __global__ void __launch_bounds__(256, 1)
     auto wait_slot = [&](int s) {
         const uint32_t bar = bars + 8u * (uint32_t)s;
         const uint32_t ph = (phase >> s) & 1u;
-        uint32_t i = 0;
-        while (ok && !mbar_try_wait(bar, ph))
-            if (++i >= kWaitLimit) ok = false;
+        if (ok) ok = mbar_wait_bounded(bar, ph, kWaitLimit);
         phase ^= 1u << s;
     };
     // first step needs all seven tiles

@@ -148,6 +148,9 @@ int fetch_results(su2g_lattice* h, int off, int n)
     if (rc) return rc;
     rc = check_cuda(h, cudaStreamSynchronize(h->stream), "synchronising");
     if (rc) return rc;
+    // a reported failure is reported once: the word is cleared and the handle stays usable
+    if (status && (rc = check_cuda(h, cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream), "clearing status")))
+        return rc;
     if (status & kStatusKpTrials)
         return set_error(h, SU2G_EDEVICE, "a heatbath link exceeded %u Kennedy-Pendleton trials", kMaxTrials);
     if (status & kStatusTmaTimeout)

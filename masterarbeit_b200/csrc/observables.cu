@@ -26,7 +26,7 @@ constexpr double kPi = 3.14159265358979323846;
 template <typename R>
 __global__ void __launch_bounds__(kBlock, 4) k_plaquette(Field<R> U, Geom g, DD* __restrict__ partials)
 {
-    R site_r = R(0);   // six plaquettes of one site, in the link precision
+    double site = 0.0;
     Site s;
     int par, h;
     if (site_cta_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) {
@@ -45,10 +45,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_plaquette(Field<R> U, Geom g, DD*
                 // Re tr U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag = 2 <U_mu(x)U_nu(x+mu), U_nu(x)U_mu(x+nu)>
                 Q<R> a = q_mul(u[mu], U.ld(nu, q, xp[mu]));
                 Q<R> b = q_mul(u[nu], U.ld(mu, q, xp[nu]));
-                site_r += q_dot(a, b);
+                site += (double)q_dot(a, b);
             }
     }
-    DD acc = dd_block_sum_d<kBlock>((double)site_r);
+    DD acc = dd_block_sum_d<kBlock>(site);
     if (threadIdx.x == 0) partials[blockIdx.x] = acc;
 }
 

@@ -99,6 +99,7 @@ _SIGS = {
     "su2g_stats_veff": (ctypes.c_int, [_DP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _I32P,
                                        _I32P, ctypes.c_int32, _DP, _DP, _DP, _DP]),
     "su2g_batch_tau_int": (ctypes.c_int, [_P, ctypes.c_int32, _DP, _I32P]),
+    "su2g_selftest_bounded_wait": (ctypes.c_int, [_P, ctypes.c_uint32]),
     "su2g_plaquette": (ctypes.c_int, [_P, _DP]),
     "su2g_ape": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32]),
     "su2g_wilson": (ctypes.c_int, [_P, _I32P, _I32P, ctypes.c_int32, _DP]),
@@ -323,6 +324,10 @@ class Lattice:
 
     def measure_release(self):
         self._check(self.lib.su2g_measure_release(self.h))
+
+    def selftest_bounded_wait(self, poll_limit=1 << 12):
+        """Run the bounded-wait diagnostic; raises Su2gError (SU2G_EDEVICE, timeout) as designed."""
+        self._check(self.lib.su2g_selftest_bounded_wait(self.h, int(poll_limit)))
 
     # -- observables
     def plaquette(self):
