@@ -209,7 +209,8 @@ int su2g_qtop(su2g_lattice *h, double *q, double *sum_abs);
  * field.  grad (may be NULL) receives, per link in the host order double[V][4][3], the su(2)
  * coefficients g of dQ under U -> exp(eps X) U, X = i x.sigma:  dQ = eps * sum g.x + O(eps^2).
  * The smeared levels are kept every `ckpt` steps (0 = ceil(sqrt(n_ape))) and recomputed in
- * between.  The handle's field is not modified. */
+ * between.  The handle's field is not modified.  The scratch (su2g_vjp_plan) comes from a memory
+ * pool of the handle that keeps it for later calls until su2g_destroy. */
 int su2g_ape_qtop_vjp(su2g_lattice *h, int32_t n_ape, double alpha, int32_t ckpt, double *q, double *grad);
 /* Levels the VJP keeps on the device and its device memory, for a given n_ape and ckpt. */
 int su2g_vjp_plan(const su2g_lattice *h, int32_t n_ape, int32_t ckpt, int32_t *levels_stored,

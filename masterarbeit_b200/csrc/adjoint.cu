@@ -21,6 +21,7 @@
 #include <cmath>
 #include <vector>
 
+#include "ape.cuh"
 #include "clover.cuh"
 #include "internal.cuh"
 
@@ -56,11 +57,8 @@ __device__ __forceinline__ void stq(double* p, size_t i, const Q<double>& q)
 // Atomic accumulation into a link of a gradient field.
 __device__ __forceinline__ void atomic_add_link(const Field<float>& G, int mu, int par, int n, const Q<float>& v)
 {
-    float* a = reinterpret_cast<float*>(G.p[mu] + ((size_t)par * G.Vh + (size_t)(n >> 1)));
-    atomicAdd(a + 0, v.c0);
-    atomicAdd(a + 1, v.c1);
-    atomicAdd(a + 2, v.c2);
-    atomicAdd(a + 3, v.c3);
+    // one 16-byte vector atomic per link
+    atomicAdd(G.p[mu] + ((size_t)par * G.Vh + (size_t)(n >> 1)), make_float4(v.c0, v.c1, v.c2, v.c3));
 }
 __device__ __forceinline__ void atomic_add_link(const Field<double>& G, int mu, int par, int n, const Q<double>& v)
 {
@@ -193,38 +191,21 @@ __global__ void __launch_bounds__(kBlock) k_qgrad_scatter(Field<R> U, Field<R> G
 // ------------------------------------------------------ one APE step back ---
 
 // v-bar(x, mu) = (Gn - u' <u', Gn>) / |v|,  v = U + alpha S,  u' = v / |v|  (all four directions).
+// The staple sums are the forward step's own (ape_staples), so v is exactly the forward's
+// pre-projection link; same site order and occupancy as the forward kernel.
 template <typename R>
-__global__ void __launch_bounds__(kBlock) k_ape_vbar(Field<R> U, Field<R> Gn, Field<R> Vbar, Geom g, R alpha)
+__global__ void __launch_bounds__(kBlock, 2) k_ape_vbar(Field<R> U, Field<R> Gn, Field<R> Vbar, Geom g, R alpha)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.V) return;
-    int par;
-    const Site s = site_lex(g, i, par);
-    const int h = i >> 1, q = par ^ 1;
-    int xp[4], xm[4];
-    Q<R> u[4];
-#pragma unroll
-    for (int mu = 0; mu < 4; ++mu) {
-        xp[mu] = s.n + up_off_rt(g, s.c, mu);
-        xm[mu] = s.n + dn_off_rt(g, s.c, mu);
-        u[mu] = U.ldh(mu, par, h);
-    }
-#pragma unroll
-    for (int mu = 0; mu < 4; ++mu) {
-        Q<R> S = q_zero<R>();
-        const int dmu = xp[mu] - s.n;
-#pragma unroll
-        for (int nu = 0; nu < 4; ++nu) {
-            if (nu == mu) continue;
-            S = q_add(S, q_mul_nd(q_mul(u[nu], U.ld(mu, q, xp[nu])), U.ld(nu, q, xp[mu])));
-            S = q_add(S, q_mul(q_mul_dn(U.ld(nu, q, xm[nu]), U.ld(mu, q, xm[nu])), U.ld(nu, par, xm[nu] + dmu)));
-        }
-        const Q<R> v = q_axpy(alpha, S, u[mu]);
+    Site s;
+    int par, h;
+    if (!site_cta_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) return;
+    ape_staples<R, SU2G_APE_ALL>(U, g, s, par, h, [&](int mu, const Q<R>& u, const Q<R>& S) {
+        const Q<R> v = q_axpy(alpha, S, u);
         const R inv = rsqrt_r(q_norm2(v));
         const Q<R> up = q_scale(v, inv);
         const Q<R> gn = Gn.ldh(mu, par, h);
         Vbar.sth(mu, par, h, q_scale(q_axpy(-q_dot(up, gn), up, gn), inv));
-    }
+    });
 }
 
 // G_k(y, l) = vbar(y, l) + alpha * sum of the 18 staple terms containing U_l(y) (derivation in the
@@ -303,16 +284,33 @@ struct FieldBuf {
     void* dirs[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
+// Scratch of one VJP from the handle's own stream-ordered pool.  The pool keeps its memory between
+// calls (release threshold: unlimited), so repeated calls do not map gigabytes of pages again; the
+// memory goes back when the handle is destroyed.
+int ensure_pool(su2g_lattice* h)
+{
+    if (h->pool) return SU2G_OK;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = h->device;
+    int rc = check_cuda(h, cudaMemPoolCreate(&h->pool, &props), "creating the scratch pool");
+    if (rc) return rc;
+    uint64_t keep = ~0ull;
+    return check_cuda(h, cudaMemPoolSetAttribute(h->pool, cudaMemPoolAttrReleaseThreshold, &keep),
+                      "configuring the scratch pool");
+}
+
 struct Arena {
     su2g_lattice* h;
     std::vector<void*> ptrs;
     int rc = SU2G_OK;
-    explicit Arena(su2g_lattice* hh) : h(hh) {}
+    explicit Arena(su2g_lattice* hh) : h(hh) { rc = ensure_pool(hh); }
     void* get(size_t bytes)
     {
         if (rc) return nullptr;
         void* p = nullptr;
-        cudaError_t e = cudaMallocAsync(&p, bytes, h->stream);
+        cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, h->pool, h->stream);
         if (e != cudaSuccess) {
             rc = check_cuda(h, e, "allocating adjoint buffers");
             return nullptr;
@@ -396,7 +394,7 @@ int vjp_t(su2g_lattice* h, int n_ape, double alpha, int c, double* q_out, double
             Field<R> Gn = make_field<R>(G[gi].dirs, g.Vh), Gk = make_field<R>(G[gi ^ 1].dirs, g.Vh);
             Field<R> Vbf = make_field<R>(Vb.dirs, g.Vh);
             launch_begin(h, SU2G_K_OTHER);
-            k_ape_vbar<R><<<grid, kBlock, 0, h->stream>>>(Uk, Gn, Vbf, g, (R)alpha);
+            k_ape_vbar<R><<<2 * (int)((g.Vh + kBlock - 1) / kBlock), kBlock, 0, h->stream>>>(Uk, Gn, Vbf, g, (R)alpha);
             k_ape_gather<R><<<dim3(grid, 4), kBlock, 0, h->stream>>>(Uk, Vbf, Gk, g, (R)alpha);
             if ((rc = launch_end(h, SU2G_K_OTHER, "smearing adjoint kernels"))) return rc;
             gi ^= 1;

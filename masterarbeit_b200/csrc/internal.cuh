@@ -140,6 +140,7 @@ struct su2g_lattice {
         const double* trace = nullptr;
         void* dirp[4] = {nullptr, nullptr, nullptr, nullptr};
     } run;
+    cudaMemPool_t pool = nullptr;      // scratch of the adjoint; keeps its memory until destroy
     su2g_meas_graph* meas = nullptr;   // graph of one su2g_measure spec
     void* meas_work = nullptr;         // measurement copy of the field and its ping-pong partner
     void* meas_alt = nullptr;

@@ -13,6 +13,7 @@
 
 #include "internal.cuh"
 #include "clover.cuh"
+#include "ape.cuh"
 
 using namespace su2g;
 
@@ -54,22 +55,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_plaquette(Field<R> U, Geom g, DD*
 
 // ------------------------------------------------------------------- APE ---
 
-__host__ __device__ constexpr bool ape_updates(int mode, int mu)
-{
-    return mode == SU2G_APE_ALL ? true : (mode == SU2G_APE_SPATIAL ? mu != 0 : mu == 0);
-}
-// Is nu a staple direction for link mu?  staples_smearing(n, dir, dt) skips kk == dir and kk == dt
-// with dt = dir (all), 0 (spatial, temporal)  (smearing.c:51, :89, :122, :155).
-__host__ __device__ constexpr bool ape_staple(int mode, int mu, int nu)
-{
-    return nu != mu && (mode == SU2G_APE_ALL ? true : nu != 0);
-}
-
-// One Jacobi step U'_mu(x) = Proj(U_mu(x) + alpha S_mu(x)) with the staples of smearing.c:42-71:
-//   S_mu(x) = sum_nu U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag + U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu).
-// The middle product P = U_mu(x+nu) U_nu(x+mu)^dag of the forward staple of mu in plane nu is
-// also the dagger of the middle product of the forward staple of nu in plane mu, so each plane's
-// P is formed once.  Reads `in`, writes only the updated directions of `out`.
+// One Jacobi step U'_mu(x) = Proj(U_mu(x) + alpha S_mu(x)) (smearing.c:74-168) with the staple
+// sums of ape_staples (ape.cuh).  Reads `in`, writes only the updated directions of `out`.
 // Resident CTAs per SM, measured at 48^4 on B200 against 2, 3 and 4: APE_all 2 (more thrash L1;
 // 255 us FP32), spatial 4 in FP32 (136 us against 164 us with 2) but 2 in FP64 (more spill),
 // temporal 4 (98 us FP32, 211 us FP64).
@@ -94,44 +81,9 @@ __global__ void __launch_bounds__(ape_block<R, MODE>(), ape_min_blocks<R, MODE>(
     Site s;
     int par, h;
     if (site_cta_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) {
-        const int q = par ^ 1;
-        Q<R> u[4], S[4];
-        int xp[4], xm[4];
-#pragma unroll
-        for (int mu = 0; mu < 4; ++mu) {
-            xp[mu] = s.n + up_off_rt(g, s.c, mu);
-            xm[mu] = s.n + dn_off_rt(g, s.c, mu);
-            S[mu] = q_zero<R>();
-            bool need = ape_updates(MODE, mu);
-#pragma unroll
-            for (int nu = 0; nu < 4; ++nu) need = need || (ape_updates(MODE, nu) && ape_staple(MODE, nu, mu));
-            if (need) u[mu] = in.ldh(mu, par, h);
-        }
-#pragma unroll
-        for (int mu = 0; mu < 4; ++mu)
-#pragma unroll
-            for (int nu = mu + 1; nu < 4; ++nu) {
-                const bool a = ape_updates(MODE, mu) && ape_staple(MODE, mu, nu);
-                const bool b = ape_updates(MODE, nu) && ape_staple(MODE, nu, mu);
-                if (!a && !b) continue;
-                const Q<R> P = q_mul_nd(in.ld(mu, q, xp[nu]), in.ld(nu, q, xp[mu]));
-                if (a) S[mu] = q_mul_add(S[mu], u[nu], P);      // U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag
-                if (b) S[nu] = q_mul_nd_add(S[nu], u[mu], P);   // U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag
-            }
-#pragma unroll
-        for (int mu = 0; mu < 4; ++mu) {
-            if (!ape_updates(MODE, mu)) continue;
-            const int dmu = xp[mu] - s.n;
-#pragma unroll
-            for (int nu = 0; nu < 4; ++nu) {
-                if (!ape_staple(MODE, mu, nu)) continue;
-                const Q<R> a = in.ld(nu, q, xm[nu]);          // U_nu(x-nu)
-                const Q<R> b = in.ld(mu, q, xm[nu]);          // U_mu(x-nu)
-                const Q<R> c = in.ld(nu, par, xm[nu] + dmu);  // U_nu(x-nu+mu)
-                S[mu] = q_mul_add(S[mu], q_mul_dn(a, b), c);
-            }
-            out.sth(mu, par, h, q_project(q_axpy(alpha, S[mu], u[mu])));
-        }
+        ape_staples<R, MODE>(in, g, s, par, h, [&](int mu, const Q<R>& u, const Q<R>& S) {
+            out.sth(mu, par, h, q_project(q_axpy(alpha, S, u)));
+        });
     }
 }
 
