@@ -230,14 +230,26 @@ __device__ __forceinline__ void gather_link(const Field<R>& U, const Field<R>& V
         const int yp = s.n + up_off_rt(g, s.c, m);   // y + m
         const int yl = s.n + dl;                     // y + l
         const int yml = ym + dl;                     // y - m + l
-        // terms over mu = m
-        acc = q_add(acc, q_mul_nd(q_mul(Vb.ld(m, par, s.n), U.ld(L, q, yp)), U.ld(m, q, yl)));
-        acc = q_add(acc, q_mul(q_mul_dn(Vb.ld(m, q, ym), U.ld(L, q, ym)), U.ld(m, par, yml)));
-        acc = q_add(acc, q_mul_nd(q_mul(U.ld(m, par, s.n), U.ld(L, q, yp)), Vb.ld(m, q, yl)));
-        acc = q_add(acc, q_mul(q_mul_dn(U.ld(m, q, ym), U.ld(L, q, ym)), Vb.ld(m, par, yml)));
-        // terms over nu = m
-        acc = q_add(acc, q_mul(q_mul_dn(U.ld(m, q, ym), Vb.ld(L, q, ym)), U.ld(m, par, yml)));
-        acc = q_add(acc, q_mul_nd(q_mul(U.ld(m, par, s.n), Vb.ld(L, q, yp)), U.ld(m, q, yl)));
+        // The six terms with a common plane share factors: with A = U_m(y), X = U_l(y+m),
+        // Xv = vbar(y+m, l), B = U_m(y+l), Vm = vbar(y, m), Vn = vbar(y+l, m)
+        //   Vm X B^dag + A Xv B^dag + A X Vn^dag = (Vm X + A Xv) B^dag + (A X) Vn^dag,
+        // and with C = U_m(y-m), Y = U_l(y-m), Yv = vbar(y-m, l), D = U_m(y-m+l),
+        // Wm = vbar(y-m, m), Wd = vbar(y-m+l, m)
+        //   Wm^dag Y D + C^dag Yv D + C^dag Y Wd = (Wm^dag Y + C^dag Yv) D + (C^dag Y) Wd:
+        // 10 products and 12 loads instead of 12 and 18.
+        {
+            const Q<R> A = U.ld(m, par, s.n), X = U.ld(L, q, yp), Xv = Vb.ld(L, q, yp);
+            const Q<R> B = U.ld(m, q, yl), Vm = Vb.ld(m, par, s.n), Vn = Vb.ld(m, q, yl);
+            const Q<R> AX = q_mul(A, X);
+            acc = q_add(acc, q_mul_nd(q_add(q_mul(Vm, X), q_mul(A, Xv)), B));
+            acc = q_add(acc, q_mul_nd(AX, Vn));
+        }
+        {
+            const Q<R> C = U.ld(m, q, ym), Y = U.ld(L, q, ym), Yv = Vb.ld(L, q, ym);
+            const Q<R> D = U.ld(m, par, yml), Wm = Vb.ld(m, q, ym), Wd = Vb.ld(m, par, yml);
+            acc = q_add(acc, q_mul(q_add(q_mul_dn(Wm, Y), q_mul_dn(C, Yv)), D));
+            acc = q_add(acc, q_mul(q_mul_dn(C, Y), Wd));
+        }
     }
     G.sth(L, par, h, q_axpy(alpha, acc, Vb.ldh(L, par, h)));
 }
