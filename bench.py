@@ -520,9 +520,10 @@ def run_ours(args, dist, dims):
         line["cpu_baseline"] = {"value": res["rates"][0], "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
                                 "sample": res["sample"], "cpu_model": res["model"], "nproc": res["nproc"]}
         if not args.no_extras:
+            # the reference's other kernels, timed beside the GPU figures of this run (CPU-baseline leg)
             ck = cpu_reference_kernels(extras, dims)
             if ck:
-                extras["cpu_reference_kernels"] = ck
+                line["cpu_baseline"]["per_kernel"] = ck
     lat.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
