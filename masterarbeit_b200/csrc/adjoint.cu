@@ -58,11 +58,11 @@ __device__ __forceinline__ void stq(double* p, size_t i, const Q<double>& q)
 __device__ __forceinline__ void atomic_add_link(const Field<float>& G, int mu, int par, int n, const Q<float>& v)
 {
     // one 16-byte vector atomic per link
-    atomicAdd(G.p[mu] + ((size_t)par * G.Vh + (size_t)(n >> 1)), make_float4(v.c0, v.c1, v.c2, v.c3));
+    atomicAdd(G.p[mu] + (unsigned)(par * G.Vh + (int)((unsigned)n >> 1)), make_float4(v.c0, v.c1, v.c2, v.c3));
 }
 __device__ __forceinline__ void atomic_add_link(const Field<double>& G, int mu, int par, int n, const Q<double>& v)
 {
-    double* a = reinterpret_cast<double*>(G.p[mu] + 2 * ((size_t)par * G.Vh + (size_t)(n >> 1)));
+    double* a = reinterpret_cast<double*>(G.p[mu] + 2u * (unsigned)(par * G.Vh + (int)((unsigned)n >> 1)));
     atomicAdd(a + 0, v.c0);
     atomicAdd(a + 1, v.c1);
     atomicAdd(a + 2, v.c2);

@@ -56,6 +56,10 @@ __device__ __forceinline__ U4 link_random(uint64_t seed, uint32_t site, uint32_t
 // Uniforms in the open interval (0,1).  FP64 keeps all 32 bits; FP32 keeps the top 23 bits, so the
 // FP32 and FP64 chains consume identical Philox words and differ only by the conversion.
 __device__ __forceinline__ double u01(uint32_t w, double) { return ((double)w + 0.5) * (1.0 / 4294967296.0); }
-__device__ __forceinline__ float u01(uint32_t w, float) { return ((float)(w >> 9) + 0.5f) * (1.0f / 8388608.0f); }
+__device__ __forceinline__ float u01(uint32_t w, float)
+{
+    // ((w >> 9) + 1/2) / 2^23 as one multiply-add: both forms are exact, so the value is the same
+    return fmaf((float)(w >> 9), 1.0f / 8388608.0f, 0.5f / 8388608.0f);
+}
 
 }  // namespace su2g

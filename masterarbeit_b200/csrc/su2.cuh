@@ -286,16 +286,17 @@ struct Field<float> {
     using ptr_t = float4*;
     float4* p[4];
     int Vh;
-    // Link at lexicographic site index n of parity par -- h = n >> 1.
-    __device__ __forceinline__ Q<float> ld(int mu, int par, int n) const { return ldh(mu, par, n >> 1); }
+    // Link at lexicographic site index n of parity par -- h = n >> 1.  Element indices are 32-bit
+    // (V <= 2^30 sites), so that an address is one wide multiply-add on the direction's base.
+    __device__ __forceinline__ Q<float> ld(int mu, int par, int n) const { return ldh(mu, par, (int)((unsigned)n >> 1)); }
     __device__ __forceinline__ Q<float> ldh(int mu, int par, int h) const
     {
-        float4 v = __ldg(p[mu] + ((size_t)par * (size_t)Vh + (size_t)h));
+        float4 v = __ldg(p[mu] + (unsigned)(par * Vh + h));
         return q_make<float>(v.x, v.y, v.z, v.w);
     }
     __device__ __forceinline__ void sth(int mu, int par, int h, const Q<float>& q) const
     {
-        p[mu][(size_t)par * (size_t)Vh + (size_t)h] = make_float4(q.c0, q.c1, q.c2, q.c3);
+        p[mu][(unsigned)(par * Vh + h)] = make_float4(q.c0, q.c1, q.c2, q.c3);
     }
 };
 
@@ -304,16 +305,16 @@ struct Field<double> {
     using ptr_t = double2*;
     double2* p[4];   // two double2 per link
     int Vh;
-    __device__ __forceinline__ Q<double> ld(int mu, int par, int n) const { return ldh(mu, par, n >> 1); }
+    __device__ __forceinline__ Q<double> ld(int mu, int par, int n) const { return ldh(mu, par, (int)((unsigned)n >> 1)); }
     __device__ __forceinline__ Q<double> ldh(int mu, int par, int h) const
     {
-        const double2* a = p[mu] + 2 * ((size_t)par * (size_t)Vh + (size_t)h);
+        const double2* a = p[mu] + 2u * (unsigned)(par * Vh + h);
         double2 x = __ldg(a), y = __ldg(a + 1);
         return q_make<double>(x.x, x.y, y.x, y.y);
     }
     __device__ __forceinline__ void sth(int mu, int par, int h, const Q<double>& q) const
     {
-        double2* a = p[mu] + 2 * ((size_t)par * (size_t)Vh + (size_t)h);
+        double2* a = p[mu] + 2u * (unsigned)(par * Vh + h);
         a[0] = make_double2(q.c0, q.c1);
         a[1] = make_double2(q.c2, q.c3);
     }

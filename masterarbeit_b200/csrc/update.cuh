@@ -32,6 +32,33 @@ __device__ __forceinline__ void kp_sincos2pi(float u, float* s, float* c)
 __device__ __forceinline__ void kp_sincos2pi(double u, double* s, double* c) { sincospi(2.0 * u, s, c); }
 __device__ __forceinline__ float kp_cos2pi(float u) { return -__cosf(6.28318530717958647692f * (u - 0.5f)); }
 __device__ __forceinline__ double kp_cos2pi(double u) { return cospi(2.0 * u); }
+// Square root of x >= 0: FP32 uses the hardware approximation (sqrt.approx.f32, relative error
+// ~2^-23), FP64 the correctly rounded one.
+__device__ __forceinline__ float kp_sqrt(float x)
+{
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ double kp_sqrt(double x) { return sqrt(x); }
+// 1/|A| and 1/(beta |A|) from |A|^2: FP32 from one hardware reciprocal square root.  |A| = 0 gives
+// k = NaN (0 * inf), which fails the k > eps test like k = 0 does.
+__device__ __forceinline__ void kp_norms(float n2, float beta, float& k, float& ik, float& ia)
+{
+    ik = rsqrtf(n2);
+    k = n2 * ik;
+    ia = __fdividef(ik, beta);
+}
+__device__ __forceinline__ void kp_norms(double n2, double beta, double& k, double& ik, double& ia)
+{
+    k = sqrt(n2);
+    ik = 1.0 / k;
+    ia = 1.0 / (k * beta);
+}
+// The FP32 logs of uniforms just below 1 may come out positive by their absolute error (~2^-21);
+// delta is clamped at 0 so that sqrt(delta (2 - delta)) stays real.  FP64 logs are exact in sign.
+__device__ __forceinline__ float kp_clamp(float d) { return fmaxf(d, 0.0f); }
+__device__ __forceinline__ double kp_clamp(double d) { return d; }
 
 // Staple sum A with U_mu(x) A = sum of the six plaquettes containing U_mu(x)  (metro.c:34-63):
 //   A = sum_{nu != mu} U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag + U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu)
@@ -96,15 +123,14 @@ __device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t se
                                               uint32_t mu, uint32_t replica, uint32_t& trials, Q<R>& out,
                                               unsigned* status, uint32_t draw_base = 0u)
 {
-    const R k = sqrt_r(q_norm2(A));
+    R k, ik, ia;   // |A|, 1/|A|, 1/alpha with alpha = |A| beta (heatbath.c:142)
+    kp_norms(q_norm2(A), beta, k, ik, ia);
     if (!(k > eps_r<R>())) {
         U4 w = link_random(seed, site, sweep, mu, draw_base | 1u, 1u, kStreamUpdate, replica);
         trials = 0;
         out = fallback_link<R>(u01(w.x, R(0)), u01(w.y, R(0)), u01(w.z, R(0)));
         return true;
     }
-    const R ik = R(1) / k;
-    const R ia = R(1) / (k * beta);          // 1/alpha, alpha = k*beta (heatbath.c:142)
     R delta;
     uint32_t trial = 0;
     for (;;) {
@@ -113,7 +139,7 @@ __device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t se
         const R u0 = u01(w.x, R(0)), u1 = u01(w.y, R(0)), u2 = u01(w.z, R(0)), u3 = u01(w.w, R(0));
         const R c = kp_cos2pi(u2);
         // X1 = -ln(u0)/alpha, X2 = -ln(u1)/alpha, delta = X2 + X1 cos^2(2 pi u2)  (heatbath.c:86-90)
-        delta = -(kp_log(u1) + kp_log(u0) * (c * c)) * ia;
+        delta = kp_clamp(-(kp_log(u1) + kp_log(u0) * (c * c)) * ia);
         if (u3 * u3 <= R(1) - R(0.5) * delta) break;   // heatbath.c:94
         if (trial >= kMaxTrials) {   // the link keeps its value and the host sees the status bit
             atomicOr(status, kStatusKpTrials);
@@ -126,10 +152,10 @@ __device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t se
     U4 w = link_random(seed, site, sweep, mu, draw_base, 1u, kStreamUpdate, replica);
     const R a0 = u01(w.x, R(0)), a1 = u01(w.y, R(0));
     const R cth = R(1) - R(2) * a1;
-    const R sth = R(2) * sqrt_r(a1 * (R(1) - a1));       // sin(acos(1 - 2 a1))
+    const R sth = R(2) * kp_sqrt(a1 * (R(1) - a1));       // sin(acos(1 - 2 a1))
     R sph, cph;
     kp_sincos2pi(a0, &sph, &cph);
-    const R len = sqrt_r(delta * (R(2) - delta));          // sqrt(1 - (1-delta)^2)
+    const R len = kp_sqrt(delta * (R(2) - delta));          // sqrt(1 - (1-delta)^2)
     Q<R> X = q_make<R>(R(1) - delta, len * sth * cph, len * sth * sph, len * cth);
     // U = X V^dag, V = A/k  (heatbath.c:140-146)
     out = q_mul_nd(X, q_scale(A, ik));

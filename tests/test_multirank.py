@@ -40,10 +40,11 @@ def test_dist_reductions_over_gloo(tmp_path):
         "d.barrier()\n"
         "out = {'rank': d.rank, 'max': d.max(10.0 + d.rank), 'sum': d.sum(1.5)}\n"
         "d.close()\n"
-        "print(json.dumps(out))\n")
+        # one file per rank: the two ranks' stdout lines can interleave under torchrun
+        f"open(os.path.join({str(tmp_path)!r}, 'rank%d.json' % out['rank']), 'w').write(json.dumps(out))\n")
     r = _torchrun([str(script)])
     assert r.returncode == 0, r.stderr[-2000:]
-    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    lines = [json.loads((tmp_path / f"rank{k}.json").read_text()) for k in range(2)]
     assert sorted(x["rank"] for x in lines) == [0, 1]
     assert all(x["max"] == 11.0 and x["sum"] == 3.0 for x in lines)
 
