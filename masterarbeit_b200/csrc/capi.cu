@@ -117,22 +117,39 @@ int ensure_partial_entries(su2g_lattice* h, size_t n)
     return ensure_partials(h, (n + kMaxPartials - 1) / kMaxPartials);
 }
 
-__global__ void k_finalize(const DD* __restrict__ partials, int nparts, int stride, double scale,
-                           double* __restrict__ out)
+// One CTA of kFinalizeBlock threads per slot.  Thread t sums partials t, t + NT, t + 2 NT, ... into
+// four compensated accumulators in turn (four independent load/add chains in flight), combines them
+// in a fixed order, and the CTA tree follows: the order is fixed, so the result is deterministic.
+// (The plaquette's 20736 partials at 48^4 took 42 us with one chain per thread of 256.)
+constexpr int kFinalizeBlock = 1024;
+
+__global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const DD* __restrict__ partials, int nparts, int stride,
+                                                             double scale, double* __restrict__ out)
 {
     const DD* p = partials + (size_t)blockIdx.x * stride;
-    DD acc = {0.0, 0.0};
-    for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc = dd_add(acc, p[i]);
-    acc = dd_block_sum<kBlock>(acc);
-    if (threadIdx.x == 0) out[blockIdx.x] = (acc.s + acc.e) * scale;
+    DD acc[4] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    int i = threadIdx.x;
+    for (; i + 3 * kFinalizeBlock < nparts; i += 4 * kFinalizeBlock) {
+        const DD a = p[i], b = p[i + kFinalizeBlock], c = p[i + 2 * kFinalizeBlock], d = p[i + 3 * kFinalizeBlock];
+        acc[0] = dd_add(acc[0], a);
+        acc[1] = dd_add(acc[1], b);
+        acc[2] = dd_add(acc[2], c);
+        acc[3] = dd_add(acc[3], d);
+    }
+    if (i < nparts) acc[0] = dd_add(acc[0], p[i]);   // at most three left for this thread
+    if (i + kFinalizeBlock < nparts) acc[1] = dd_add(acc[1], p[i + kFinalizeBlock]);
+    if (i + 2 * kFinalizeBlock < nparts) acc[2] = dd_add(acc[2], p[i + 2 * kFinalizeBlock]);
+    DD v = dd_add(dd_add(acc[0], acc[1]), dd_add(acc[2], acc[3]));
+    v = dd_block_sum<kFinalizeBlock>(v);
+    if (threadIdx.x == 0) out[blockIdx.x] = (v.s + v.e) * scale;
 }
 
 int finalize(su2g_lattice* h, int nparts, int nslots, double scale, int out_off, int stride)
 {
     if (out_off + nslots > kOutSlots) return set_error(h, SU2G_EINVAL, "too many result slots");
     launch_begin(h, SU2G_K_REDUCE);
-    k_finalize<<<nslots, kBlock, 0, h->stream>>>(h->partials, nparts, stride > 0 ? stride : kMaxPartials, scale,
-                                                  h->d_out + out_off);
+    k_finalize<<<nslots, kFinalizeBlock, 0, h->stream>>>(h->partials, nparts, stride > 0 ? stride : kMaxPartials,
+                                                          scale, h->d_out + out_off);
     return launch_end(h, SU2G_K_REDUCE, "finalize reduction");
 }
 
