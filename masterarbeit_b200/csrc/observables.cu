@@ -204,10 +204,40 @@ __global__ void __launch_bounds__(kBlock) k_wilson(Field<R> U, Geom g, int r0, i
 // it is read, not rebuilt, which removes the longest product chain of the per-site form.
 constexpr int kWilsonColMaxThreads = 512;
 
+// Accumulation of the column kernel's loop terms in shared memory.  FP32: the 32 lanes' terms are
+// summed in the link precision (one shuffle per step; its rounding, ~1e-7 of a warp sum, is far
+// below the FP32 links' own) and lane 0 adds the warp sum to the warp's slot.  FP64: every thread
+// adds its own term to its own slot (no shuffles; the FP64 shuffle pairs cost more than the larger
+// slot array).  A slot adds a few hundred terms (3 directions x the CTA's tiles) in plain FP64; the
+// slots of all warps or threads and of all CTAs are then summed compensated, in a fixed order.
+// Slot layout: [r][T - tlo][owner], owner = warp (FP32) or thread (FP64).
+template <typename R>
+__host__ __device__ constexpr bool wilson_thread_slots() { return sizeof(R) == 8; }
+
+template <typename R>
+__device__ __forceinline__ size_t wilson_slot(int r, int ti, int nT, int warp, int rc)
+{
+    (void)rc;
+    return wilson_thread_slots<R>() ? ((size_t)r * nT + ti) * blockDim.x + threadIdx.x
+                                    : ((size_t)r * nT + ti) * (blockDim.x >> 5) + warp;
+}
+
+template <typename R>
+__device__ __forceinline__ void wilson_acc(double* __restrict__ wacc, R w, size_t slot, int lane)
+{
+    if (wilson_thread_slots<R>()) {
+        wacc[slot] += (double)w;
+    } else {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (lane == 0) wacc[slot] += (double)w;
+    }
+}
+
 template <typename R, int K, int RC>
 __device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g, Q<R>* __restrict__ line,
-                                               DD* __restrict__ wacc, int sw, int t, int j, int s, bool valid, int r0,
-                                               int tlo, int thi)
+                                               double* __restrict__ wacc, int sw, int t, int j, int s, bool valid,
+                                               int r0, int tlo, int thi)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nT = thi - tlo + 1;
     int par;
@@ -240,15 +270,8 @@ __device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g,
         const Q<R>* other = line + (size_t)(tt * sw + j) * RC;   // S_{r0+r}(x + T t)
 #pragma unroll
         for (int r = 0; r < RC; ++r) {
-            // the 32 lanes' terms are summed in the link precision (FP32: one shuffle per step; its
-            // rounding, ~1e-7 of a warp sum, is far below the FP32 links' own), then compensated FP64
-            R w = valid ? q_dot(q_mul(TX, other[r]), q_mul(own[r], TR[r])) : R(0);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-            if (lane == 0) {
-                DD* slot = wacc + ((size_t)warp * RC + r) * nT + (T - tlo);
-                *slot = dd_add(*slot, (double)w);
-            }
+            const R w = valid ? q_dot(q_mul(TX, other[r]), q_mul(own[r], TR[r])) : R(0);
+            wilson_acc<R>(wacc, w, wilson_slot<R>(r, T - tlo, nT, warp, RC), lane);
         }
     }
     __syncthreads();   // `line` is overwritten next
@@ -261,8 +284,9 @@ __global__ void __launch_bounds__(kWilsonColMaxThreads, 1) k_wilson_col(Field<R>
     extern __shared__ __align__(16) unsigned char wsm[];
     Q<R>* line = (Q<R>*)wsm;
     const int nwarps = blockDim.x >> 5, nT = thi - tlo + 1;
-    DD* wacc = (DD*)(wsm + (size_t)blockDim.x * RC * sizeof(Q<R>));
-    for (int i = threadIdx.x; i < nwarps * RC * nT; i += blockDim.x) wacc[i] = DD{0.0, 0.0};
+    double* wacc = (double*)(wsm + (size_t)blockDim.x * RC * sizeof(Q<R>));
+    const int owners = wilson_thread_slots<R>() ? (int)blockDim.x : nwarps;
+    for (int i = threadIdx.x; i < owners * RC * nT; i += blockDim.x) wacc[i] = 0.0;
     __syncthreads();
     const int t = threadIdx.x / sw, j = threadIdx.x % sw;
     const int stot = g.S[0], ntiles = (stot + sw - 1) / sw;
@@ -278,7 +302,7 @@ __global__ void __launch_bounds__(kWilsonColMaxThreads, 1) k_wilson_col(Field<R>
     for (int i = threadIdx.x; i < RC * nT; i += blockDim.x) {
         const int r = i / nT, ti = i % nT;
         DD v = {0.0, 0.0};
-        for (int w = 0; w < nwarps; ++w) v = dd_add(v, wacc[((size_t)w * RC + r) * nT + ti]);
+        for (int w = 0; w < owners; ++w) v = dd_add(v, wacc[((size_t)r * nT + ti) * owners + w]);
         partials[(size_t)(r * kWilsonTChunk + ti) * kMaxPartials + blockIdx.x] = v;
     }
 }
@@ -307,7 +331,8 @@ int wilson_col_width(const Geom& g, int min_threads = 256)
 template <typename R, int RC>
 size_t wilson_col_smem(int threads, int nT)
 {
-    return (size_t)threads * RC * sizeof(Q<R>) + (size_t)(threads / 32) * RC * nT * sizeof(DD);
+    const int owners = wilson_thread_slots<R>() ? threads : threads / 32;
+    return (size_t)threads * RC * sizeof(Q<R>) + (size_t)owners * RC * nT * sizeof(double);
 }
 
 // --------------------------------------------------- topological charge ---
