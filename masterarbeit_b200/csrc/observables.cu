@@ -349,9 +349,10 @@ __device__ __forceinline__ double qtop_density(const Field<R>& U, const Geom& g,
 }
 
 // One site per thread; CTA partials of q and |q| at partials[b] and partials[gridDim.x + b].
-// FP32: two resident CTAs per SM (at most 128 registers a thread); FP64 needs more registers.
+// Resident CTAs per SM: three in FP32 (80 registers, no spill) and two in FP64 (126), measured at 48^4
+// on B200 against two and one: 282.9 against 267.6 Q/s in FP32, ~166 against ~157 in FP64.
 template <typename R>
-__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 2 : 1) k_qtop(Field<R> U, Geom g, DD* __restrict__ partials)
+__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 3 : 2) k_qtop(Field<R> U, Geom g, DD* __restrict__ partials)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double d = 0.0;
