@@ -254,14 +254,15 @@ __device__ __forceinline__ void gather_link(const Field<R>& U, const Field<R>& V
     G.sth(L, par, h, q_axpy(alpha, acc, Vb.ldh(L, par, h)));
 }
 
+// One link per thread, blockIdx.y = its direction.  CTA 2k takes parity 0 and CTA 2k+1 parity 1 of
+// the same run of half-volume indices (site_cta_pair), so that every warp reads consecutive links
+// of one parity array.
 template <typename R>
 __global__ void __launch_bounds__(kBlock) k_ape_gather(Field<R> U, Field<R> Vb, Field<R> G, Geom g, R alpha)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.V) return;
-    int par;
-    const Site s = site_lex(g, i, par);
-    const int h = i >> 1;
+    Site s;
+    int par, h;
+    if (!site_cta_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) return;
     switch (blockIdx.y) {
         case 0: gather_link<R, 0>(U, Vb, G, g, s, par, h, alpha); break;
         case 1: gather_link<R, 1>(U, Vb, G, g, s, par, h, alpha); break;
@@ -407,7 +408,8 @@ int vjp_t(su2g_lattice* h, int n_ape, double alpha, int c, double* q_out, double
             Field<R> Vbf = make_field<R>(Vb.dirs, g.Vh);
             launch_begin(h, SU2G_K_OTHER);
             k_ape_vbar<R><<<2 * (int)((g.Vh + kBlock - 1) / kBlock), kBlock, 0, h->stream>>>(Uk, Gn, Vbf, g, (R)alpha);
-            k_ape_gather<R><<<dim3(grid, 4), kBlock, 0, h->stream>>>(Uk, Vbf, Gk, g, (R)alpha);
+            k_ape_gather<R><<<dim3(2 * (int)((g.Vh + kBlock - 1) / kBlock), 4), kBlock, 0, h->stream>>>(Uk, Vbf, Gk, g,
+                                                                                                      (R)alpha);
             if ((rc = launch_end(h, SU2G_K_OTHER, "smearing adjoint kernels"))) return rc;
             gi ^= 1;
         }
