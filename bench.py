@@ -382,13 +382,17 @@ def run_ours(args, dist, dims):
 
     for _ in range(W):
         step()
-    lat.profile(True)
     clocks = Clocks(dist.local)
     dist.barrier()
     lat.synchronize()
     clocks.start()
-    ms = time_steps(lat, K, step)
+    ms = time_steps(lat, K, step)   # the headline: plain calls, as a user makes them
     clk = clocks.stop()
+    # the same K steps again with every launch bracketed by CUDA events: the per-kernel durations
+    # of the roofline (the events add a few microseconds between launches, so not the headline)
+    lat.profile(True)
+    dist.barrier()
+    ms_instr = time_steps(lat, K, step)
     prof = lat.profile_read()
     lat.profile(False)
     dist.barrier()
@@ -421,7 +425,10 @@ def run_ours(args, dist, dims):
                      "frac": (dom["achieved_gbs"] / peak) if dom else None, "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6650 GB/s",
-                     "alg_bytes_per_launch": dom.get("alg_bytes_per_launch"), "per_kernel": roof},
+                     "alg_bytes_per_launch": dom.get("alg_bytes_per_launch"), "per_kernel": roof,
+                     "timing": "per-kernel CUDA-event durations from a second pass of the same K steps with "
+                               "every launch bracketed by events; value and ms_per_step from the plain pass",
+                     "ms_per_step_with_events": ms_instr / K},
         "gpu_launches": launches,
         "clocks": clk,
     }
