@@ -22,11 +22,15 @@ using namespace su2g;
 
 namespace {
 
-// At least 4 resident CTAs per SM (at most 64 registers a thread): measured at 48^4 on B200 against
-// 1, 2, 3 and 6, it is the fastest for both kinds and precisions (OR FP32 64 us, 92 % of the
-// measured copy bandwidth, against 79 us unbounded).
+// 32 resident warps per SM (at most 64 registers a thread): measured at 48^4 on B200 against 8, 16,
+// 24 and 48, it is the fastest for both kinds and precisions (OR FP32 64 us against 79 us unbounded).
+// Overrelaxation runs them as eight 128-thread CTAs (65.8 against 66.7 us with four of 256: finer
+// CTAs shorten the pass's tail); the heatbath keeps 256-thread CTAs for its acceptance reduction.
+template <int KIND>
+constexpr int update_block() { return KIND == SU2G_OVERRELAX ? 128 : kBlock; }
+
 template <typename R, int MU, int KIND>
-__global__ void __launch_bounds__(kBlock, 4) k_update(Field<R> U, Geom g, int par, R beta, uint64_t seed, uint32_t sweep,
+__global__ void __launch_bounds__(update_block<KIND>(), 1024 / update_block<KIND>()) k_update(Field<R> U, Geom g, int par, R beta, uint64_t seed, uint32_t sweep,
                                                    const uint32_t* __restrict__ sweep_base, uint32_t replica,
                                                    double* __restrict__ acc_sum, unsigned* __restrict__ status)
 {
@@ -139,10 +143,10 @@ void launch_update_t(su2g_lattice* h, int mu, int par, uint32_t sweep, const uin
     Field<R> U = make_field<R>(h->dirp, h->g.Vh);
     const R beta = (R)h->beta;
     switch (mu) {
-        case 0: k_update<R, 0, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
-        case 1: k_update<R, 1, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
-        case 2: k_update<R, 2, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
-        default: k_update<R, 3, KIND><<<grid, kBlock, 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        case 0: k_update<R, 0, KIND><<<grid, update_block<KIND>(), 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        case 1: k_update<R, 1, KIND><<<grid, update_block<KIND>(), 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        case 2: k_update<R, 2, KIND><<<grid, update_block<KIND>(), 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        default: k_update<R, 3, KIND><<<grid, update_block<KIND>(), 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
     }
 }
 
@@ -152,7 +156,8 @@ int su2g::launch_update(su2g_lattice* h, int kind, int mu, int par, uint32_t swe
                         const uint32_t* base)
 {
     const int cls = kind == SU2G_HEATBATH ? SU2G_K_HEATBATH : SU2G_K_OVERRELAX;
-    const int grid = (int)((h->g.Vh + kBlock - 1) / kBlock);
+    const int nt = kind == SU2G_HEATBATH ? update_block<SU2G_HEATBATH>() : update_block<SU2G_OVERRELAX>();
+    const int grid = (int)((h->g.Vh + nt - 1) / nt);
     launch_begin(h, cls);
     if (h->prec == SU2G_FP32) {
         if (kind == SU2G_HEATBATH) launch_update_t<float, SU2G_HEATBATH>(h, mu, par, sweep, base, acc_sum, grid);
