@@ -57,20 +57,19 @@ __global__ void __launch_bounds__(kBlock, 4) k_plaquette(Field<R> U, Geom g, DD*
 
 // One Jacobi step U'_mu(x) = Proj(U_mu(x) + alpha S_mu(x)) (smearing.c:74-168) with the staple
 // sums of ape_staples (ape.cuh).  Reads `in`, writes only the updated directions of `out`.
-// Resident CTAs per SM, measured at 48^4 on B200 against 2, 3 and 4: APE_all 2 (more thrash L1;
-// 255 us FP32), spatial 4 in FP32 (136 us against 164 us with 2) but 2 in FP64 (more spill),
-// temporal 4 (98 us FP32, 211 us FP64).
-// FP32 APE_all runs 128-thread CTAs, five per SM (at most 102 registers): 239 us against 254 us with
-// two 256-thread CTAs (the scheduler holding 4 warps of a 128-register kernel); FP64 spills there.
+// Resident CTAs per SM, measured at 48^4 on B200: FP32 APE_all five 128-thread CTAs (at most 102
+// registers; 239 us against 254 us with two 256-thread CTAs, 243 us with six); FP32 spatial and
+// temporal eight 128-thread CTAs (131.4 us spatial against 132.6 us with four of 256 and 164 us with
+// two); FP64 two 256-thread CTAs (more spill).
 template <typename R, int MODE>
 constexpr int ape_min_blocks()
 {
-    return MODE == SU2G_APE_ALL ? (sizeof(R) == 4 ? 5 : 2) : (sizeof(R) == 4 || MODE == SU2G_APE_TEMPORAL ? 4 : 2);
+    return MODE == SU2G_APE_ALL ? (sizeof(R) == 4 ? 5 : 2) : (sizeof(R) == 4 ? 8 : (MODE == SU2G_APE_TEMPORAL ? 4 : 2));
 }
 template <typename R, int MODE>
 constexpr int ape_block()
 {
-    return MODE == SU2G_APE_ALL && sizeof(R) == 4 ? 128 : kBlock;
+    return sizeof(R) == 4 ? 128 : kBlock;
 }
 
 template <typename R, int MODE>

@@ -24,10 +24,10 @@ namespace {
 
 // 32 resident warps per SM (at most 64 registers a thread): measured at 48^4 on B200 against 8, 16,
 // 24 and 48, it is the fastest for both kinds and precisions (OR FP32 64 us against 79 us unbounded).
-// Overrelaxation runs them as eight 128-thread CTAs (65.8 against 66.7 us with four of 256: finer
-// CTAs shorten the pass's tail); the heatbath keeps 256-thread CTAs for its acceptance reduction.
+// Both kinds run them as eight 128-thread CTAs: finer CTAs shorten the pass's tail (OR 65.8 against
+// 66.7 us, HB 86.7 against 88.1 us with four CTAs of 256).
 template <int KIND>
-constexpr int update_block() { return KIND == SU2G_OVERRELAX ? 128 : kBlock; }
+constexpr int update_block() { return 128; }
 
 template <typename R, int MU, int KIND>
 __global__ void __launch_bounds__(update_block<KIND>(), 1024 / update_block<KIND>()) k_update(Field<R> U, Geom g, int par, R beta, uint64_t seed, uint32_t sweep,
@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(update_block<KIND>(), 1024 / update_block<KIND
     }
     if (KIND == SU2G_HEATBATH && acc_sum) {
         DD v = {acc_thread, 0.0};
-        v = dd_block_sum<kBlock>(v);
+        v = dd_block_sum<update_block<KIND>()>(v);
         if (threadIdx.x == 0) atomicAdd(acc_sum, v.s + v.e);
     }
 }
