@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_plaquette(Field<R> U, Geom g, DD*
 // Resident CTAs per SM, measured at 48^4 on B200: FP32 APE_all five 128-thread CTAs (at most 102
 // registers; 239 us against 254 us with two 256-thread CTAs, 243 us with six); FP32 spatial and
 // temporal eight 128-thread CTAs (131.4 us spatial against 132.6 us with four of 256 and 164 us with
-// two); FP64 two 256-thread CTAs (more spill).
+// two); FP64 256-thread CTAs, two for all and spatial (more spill) and four for temporal.
 template <typename R, int MODE>
 constexpr int ape_min_blocks()
 {
