@@ -76,10 +76,12 @@ template <typename R, int MODE>
 __global__ void __launch_bounds__(ape_block<R, MODE>(), ape_min_blocks<R, MODE>()) k_ape(Field<R> in, Field<R> out,
                                                                                         Geom g, R alpha)
 {
-    // one site per thread; CTAs dispatched in order, alternating parity over the same h run
+    // one site per thread; CTAs dispatched in order, warps alternating parity over the same h run
+    // (so that both parities of a region share an L1: FP32 APE_all 237.8 against 240.7 us, spatial
+    // 129.1 against 131.6 us, FP64 spatial 355 against 367 us with parity-alternating CTAs)
     Site s;
     int par, h;
-    if (site_cta_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) {
+    if (site_warp_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) {
         ape_staples<R, MODE>(in, g, s, par, h, [&](int mu, const Q<R>& u, const Q<R>& S) {
             out.sth(mu, par, h, q_project(q_axpy(alpha, S, u)));
         });
@@ -385,7 +387,7 @@ template <typename R, int MODE>
 void launch_ape_t(su2g_lattice* h, const Field<R>& in, const Field<R>& out, R alpha)
 {
     constexpr int block = ape_block<R, MODE>();
-    const int grid = 2 * (int)((h->g.Vh + block - 1) / block);   // CTA pairs over the same h run
+    const int grid = (int)((2 * (long long)h->g.Vh + block - 1) / block);   // warp pairs over the same h run
     k_ape<R, MODE><<<grid, block, 0, h->stream>>>(in, out, h->g, alpha);
 }
 

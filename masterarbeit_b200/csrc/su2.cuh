@@ -251,6 +251,21 @@ __device__ __forceinline__ bool site_cta_pair(const Geom& g, int cta, int tid, i
     return true;
 }
 
+// Site visited by thread `tid` of CTA `cta` when the warps of a CTA alternate parity over the same
+// run of h: warp 2k takes parity 0 and warp 2k+1 parity 1 of h = cta ntid/2 + 32k .. + 31.  Every warp
+// still reads consecutive links of one parity array, and both parities of a region are loaded by
+// the same SM, so a site's neighbours of the other parity are often in its L1.
+// Grid: ceil(Vh / (ntid / 2)); ntid a multiple of 64.
+__device__ __forceinline__ bool site_warp_pair(const Geom& g, int cta, int tid, int ntid, Site& s, int& par, int& h)
+{
+    const int w = tid >> 5;
+    par = w & 1;
+    h = cta * (ntid >> 1) + (w >> 1) * 32 + (tid & 31);
+    if (h >= g.Vh) return false;
+    s = site_of(g, par, h);
+    return true;
+}
+
 // Lexicographic index offset of the +mu / -mu neighbour of a site (periodic).
 template <int MU>
 __device__ __forceinline__ int up_off(const Geom& g, const Site& s)
