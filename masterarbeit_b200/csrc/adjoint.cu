@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_ape_vbar(Field<R> U, Field<R> Gn,
 {
     Site s;
     int par, h;
-    if (!site_cta_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) return;
+    if (!site_warp_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) return;
     ape_staples<R, SU2G_APE_ALL>(U, g, s, par, h, [&](int mu, const Q<R>& u, const Q<R>& S) {
         const Q<R> v = q_axpy(alpha, S, u);
         const R inv = rsqrt_r(q_norm2(v));
@@ -254,15 +254,15 @@ __device__ __forceinline__ void gather_link(const Field<R>& U, const Field<R>& V
     G.sth(L, par, h, q_axpy(alpha, acc, Vb.ldh(L, par, h)));
 }
 
-// One link per thread, blockIdx.y = its direction.  CTA 2k takes parity 0 and CTA 2k+1 parity 1 of
-// the same run of half-volume indices (site_cta_pair), so that every warp reads consecutive links
-// of one parity array.
+// One link per thread, blockIdx.y = its direction.  Warp 2k takes parity 0 and warp 2k+1 parity 1
+// of the same 32 half-volume indices (site_warp_pair): every warp reads consecutive links of one
+// parity array, and both parities of a region are loaded by the same SM.
 template <typename R>
 __global__ void __launch_bounds__(kBlock) k_ape_gather(Field<R> U, Field<R> Vb, Field<R> G, Geom g, R alpha)
 {
     Site s;
     int par, h;
-    if (!site_cta_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) return;
+    if (!site_warp_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) return;
     switch (blockIdx.y) {
         case 0: gather_link<R, 0>(U, Vb, G, g, s, par, h, alpha); break;
         case 1: gather_link<R, 1>(U, Vb, G, g, s, par, h, alpha); break;
