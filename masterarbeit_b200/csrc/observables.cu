@@ -355,13 +355,11 @@ __device__ __forceinline__ double qtop_density(const Field<R>& U, const Geom& g,
 template <typename R>
 __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 3 : 2) k_qtop(Field<R> U, Geom g, DD* __restrict__ partials)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // parities paired per warp (site_warp_pair); grid ceil(V / kBlock)
+    Site s;
+    int par, h;
     double d = 0.0;
-    if (i < g.V) {
-        int par;
-        const Site s = site_lex(g, i, par);
-        d = qtop_density<R>(U, g, s, par);
-    }
+    if (site_warp_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) d = qtop_density<R>(U, g, s, par);
     DD acc = dd_block_sum_d<kBlock>(d);
     DD aabs = dd_block_sum_d<kBlock>(fabs(d));
     if (threadIdx.x == 0) {
