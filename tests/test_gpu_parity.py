@@ -86,6 +86,25 @@ def test_qtop_after_ape(golden, lat):
                 assert abs(q - qref) <= tol * sabs, (prec, N, q, qref, sabs)
 
 
+@pytest.mark.parametrize("dims", [(4, 4, 6, 6), (6, 6, 4, 10), (4, 6, 8, 10)])
+def test_ape_and_qtop_on_ragged_geometries(dims):
+    """Half volumes that are not whole multiples of a CTA's run of sites (288 and 720 against the
+    64 sites of a 128-thread CTA whose warps alternate parity; 960 against the 128 sites of the
+    FP64 CTAs), so the last CTA of the APE and charge kernels is partly empty: APE in every mode,
+    then Q, against the oracle on the same uploaded Haar field, in FP64 and FP32."""
+    U = O.start(dims, "haar", 17)
+    for mode in ("all", "spatial", "temporal"):
+        ref = O.ape(dims, U, 3, 0.4, mode)
+        qref, _ = O.qtop(dims, ref)
+        for prec, tol, qtol in (("fp64", 1e-13, 1e-12), ("fp32", 2e-6, 2e-5)):
+            L = Lattice(dims, precision=prec)
+            L.upload(U)
+            L.ape(3, 0.4, mode)
+            assert np.max(np.abs(L.download() - ref)) <= tol, (prec, mode)
+            q, sabs = L.qtop(with_abs=True)
+            assert abs(q - qref) <= qtol * sabs, (prec, mode, q, qref)
+
+
 @pytest.mark.parametrize("lat", LATS)
 def test_heatbath_matches_reference_link_by_link(golden, lat):
     """GPU checkerboard heatbath vs the reference's localHeatbathUpdate on the same Philox uniforms."""
