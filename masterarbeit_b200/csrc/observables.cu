@@ -216,9 +216,8 @@ template <typename R>
 __host__ __device__ constexpr bool wilson_thread_slots() { return sizeof(R) == 8; }
 
 template <typename R>
-__device__ __forceinline__ size_t wilson_slot(int r, int ti, int nT, int warp, int rc)
+__device__ __forceinline__ size_t wilson_slot(int r, int ti, int nT, int warp)
 {
-    (void)rc;
     return wilson_thread_slots<R>() ? ((size_t)r * nT + ti) * blockDim.x + threadIdx.x
                                     : ((size_t)r * nT + ti) * (blockDim.x >> 5) + warp;
 }
@@ -272,7 +271,7 @@ __device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g,
 #pragma unroll
         for (int r = 0; r < RC; ++r) {
             const R w = valid ? q_dot(q_mul(TX, other[r]), q_mul(own[r], TR[r])) : R(0);
-            wilson_acc<R>(wacc, w, wilson_slot<R>(r, T - tlo, nT, warp, RC), lane);
+            wilson_acc<R>(wacc, w, wilson_slot<R>(r, T - tlo, nT, warp), lane);
         }
     }
     __syncthreads();   // `line` is overwritten next
