@@ -96,7 +96,8 @@ __global__ void __launch_bounds__(256, 1)
     }
     __syncthreads();
     // tiles in time order; slot phases flip per completed tile
-    uint32_t phase = 0;   // bit s = parity of slot s's next completion
+    uint32_t phase = 0;     // bit s = parity of slot s's next completion
+    uint32_t pending = 0;   // thread 0: slots whose copies have been issued and not yet seen complete
     if (threadIdx.x == 0) {
         // t = -1 is plane LT-1; ring slots are indexed with t + 4*LT (>= 0)
         issue_tile(in, g, tg, slots, bars, sC(4 * LT - 1), LT - 1, x, y0);
@@ -106,6 +107,8 @@ __global__ void __launch_bounds__(256, 1)
         issue_tile(in, g, tg, slots, bars, sP(3 * LT + 0), 0, xpl, y0);
         issue_tile(in, g, tg, slots, bars, sM(3 * LT + 0), 0, xmn, y0);
         issue_tile(in, g, tg, slots, bars, sM(3 * LT + 1), wrap(1, LT), xmn, y0);
+        pending = (1u << sC(4 * LT - 1)) | (1u << sC(4 * LT)) | (1u << sC(4 * LT + 1)) | (1u << sP(3 * LT - 1)) |
+                  (1u << sP(3 * LT)) | (1u << sM(3 * LT)) | (1u << sM(3 * LT + 1));
     }
     // thread -> output site (row yl, z) of the current plane
     const int L3 = g.L[3];
@@ -121,7 +124,19 @@ __global__ void __launch_bounds__(256, 1)
         const uint32_t bar = bars + 8u * (uint32_t)s;
         const uint32_t ph = (phase >> s) & 1u;
         if (ok) ok = mbar_wait_bounded(bar, ph, kWaitLimit);
+        if (ok) pending &= ~(1u << s);
         phase ^= 1u << s;
+    };
+    // On a timeout the CTA stops; before it exits, thread 0 waits (again bounded) for the copies it
+    // issued that have not been seen to complete, so that no bulk copy into this CTA's shared memory
+    // is left in flight.  Every issued slot has had exactly one wait_slot since its issue, which
+    // flipped its phase bit, so the phase still owed is the flipped-back one.
+    auto give_up = [&]() {
+        if (threadIdx.x == 0) {
+            for (int s = 0; s < kSlots; ++s)
+                if (pending & (1u << s)) mbar_wait_bounded(bars + 8u * (uint32_t)s, ((phase >> s) & 1u) ^ 1u, kWaitLimit);
+            atomicOr(status, kStatusTmaTimeout);
+        }
     };
     // first step needs all seven tiles
     wait_slot(sC(4 * LT - 1));
@@ -132,7 +147,7 @@ __global__ void __launch_bounds__(256, 1)
     wait_slot(sM(3 * LT));
     wait_slot(sM(3 * LT + 1));
     if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) atomicOr(status, kStatusTmaTimeout);
+        give_up();
         return;
     }
 
@@ -143,6 +158,7 @@ __global__ void __launch_bounds__(256, 1)
             issue_tile(in, g, tg, slots, bars, sC(tt + 2), wrap(t + 2, LT), x, y0);
             issue_tile(in, g, tg, slots, bars, sP(t3 + 1), wrap(t + 1, LT), xpl, y0);
             issue_tile(in, g, tg, slots, bars, sM(t3 + 2), wrap(t + 2, LT), xmn, y0);
+            pending |= (1u << sC(tt + 2)) | (1u << sP(t3 + 1)) | (1u << sM(t3 + 2));
         }
         if (active) {
             // link loader: tile (dt, dx) relative to (t, x), row offset dy, z offset dz
@@ -199,7 +215,7 @@ __global__ void __launch_bounds__(256, 1)
             wait_slot(sP(t3 + 1));
             wait_slot(sM(t3 + 2));
             if (__syncthreads_or(!ok)) {
-                if (threadIdx.x == 0) atomicOr(status, kStatusTmaTimeout);
+                give_up();
                 return;
             }
         }

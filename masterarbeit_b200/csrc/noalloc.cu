@@ -33,7 +33,9 @@ void* g_scratch_addr[kMaxDevices] = {nullptr};
 
 // Device address of g_noalloc_scratch on the current device.  In host code the array's name is
 // only a host-side stand-in, so the address is looked up once per device (with that device
-// current) and cached; a kernel is always given this looked-up address.
+// current) and cached; a kernel is always given this looked-up address.  The cache lives as long
+// as the process: after cudaDeviceReset the module is loaded again and the array may move, so a
+// program that resets a device must not call this entry point afterwards (restart the process).
 int scratch_address(int dev, void** out)
 {
     if (dev < 0 || dev >= kMaxDevices)
@@ -140,6 +142,24 @@ extern "C" int su2g_ape_inplace_noalloc(double* links, const int32_t dims[4], in
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess)
         return set_error(nullptr, SU2G_ECUDA, "su2g_ape_inplace_noalloc: %s", cudaGetErrorString(e));
+    // The kernels read and write the field as double2, so it must be 16-byte aligned device (or
+    // managed) memory of the current device.  Callers hand in sub-allocations of their own pools,
+    // so a bad pointer is refused here instead of faulting on the GPU.  Neither check allocates.
+    if (((uintptr_t)links & 15u) != 0)
+        return set_error(nullptr, SU2G_EINVAL,
+                         "su2g_ape_inplace_noalloc: field pointer %p is not 16-byte aligned", (void*)links);
+    cudaPointerAttributes pa;
+    e = cudaPointerGetAttributes(&pa, links);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(nullptr, SU2G_EINVAL, "su2g_ape_inplace_noalloc: cannot query pointer %p: %s", (void*)links,
+                         cudaGetErrorString(e));
+    }
+    if ((pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged) ||
+        (pa.type == cudaMemoryTypeDevice && pa.device != dev))
+        return set_error(nullptr, SU2G_EINVAL,
+                         "su2g_ape_inplace_noalloc: field pointer %p is not device memory of the current device %d",
+                         (void*)links, dev);
     void* scratch = nullptr;
     int rc = scratch_address(dev, &scratch);
     if (rc) return rc;

@@ -177,17 +177,13 @@ __global__ void __launch_bounds__(kBlock) k_wilson(Field<R> U, Geom g, int r0, i
         int par;
         const Site s = site_lex(g, ii, par);
         DD* acc = &wacc[warp][0];
-        // Lanes past the end recompute a valid site with an empty record window (tlo > thi), so
-        // that every lane takes part in the warp shuffles.
-        if (valid) {
-            wilson_site<R, 1, RC>(U, g, s, par, r0, tlo, thi, acc);
-            wilson_site<R, 2, RC>(U, g, s, par, r0, tlo, thi, acc);
-            wilson_site<R, 3, RC>(U, g, s, par, r0, tlo, thi, acc);
-        } else {
-            wilson_site<R, 1, RC>(U, g, s, par, r0, thi + 1, thi, acc);
-            wilson_site<R, 2, RC>(U, g, s, par, r0, thi + 1, thi, acc);
-            wilson_site<R, 3, RC>(U, g, s, par, r0, thi + 1, thi, acc);
-        }
+        // Lanes past the end recompute a valid site with an empty record window (tlo > thi).  Every
+        // lane makes the same calls, so each full-mask shuffle inside is one instruction executed
+        // by the whole warp.
+        const int tlo_lane = valid ? tlo : thi + 1;
+        wilson_site<R, 1, RC>(U, g, s, par, r0, tlo_lane, thi, acc);
+        wilson_site<R, 2, RC>(U, g, s, par, r0, tlo_lane, thi, acc);
+        wilson_site<R, 3, RC>(U, g, s, par, r0, tlo_lane, thi, acc);
     }
     __syncthreads();
     // fixed-order sum over warps, one partial per slot

@@ -12,14 +12,15 @@
 # build folder to patch the extents, because modules.h includes "headers.h" from its own
 # directory.  Outputs go to masterarbeit_b200/shim/_build/<dims>/.
 #
-# usage: build_dropin.sh [REF_ROOT] [DIMS ...]
+# usage: build_dropin.sh REF_ROOT [DIMS ...]
 set -euo pipefail
 
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 PKG="$(dirname "$HERE")"
 REPO="$(dirname "$PKG")"
-REF="${1:-/root/reference}"
-shift || true
+[ $# -ge 1 ] || { echo "usage: build_dropin.sh REF_ROOT [DIMS ...]" >&2; exit 2; }
+REF="$1"
+shift
 DIMS=("$@")
 [ ${#DIMS[@]} -eq 0 ] && DIMS=(8x8x8x8)
 LGT="$REF/LGT_Code"

@@ -12,12 +12,13 @@
 # Flags follow LGT_Code/main/Makefile:64-69,:85-98 (gcc -O3 -Wall -mcmodel=large).
 # Shipped objects and binaries of the reference are never used.
 #
-# usage: oracle/build_ref.sh [REF_ROOT] [DIMS ...]     DIMS like 8x8x8x8 (T x X x Y x Z)
+# usage: oracle/build_ref.sh REF_ROOT [DIMS ...]     DIMS like 8x8x8x8 (T x X x Y x Z)
 set -euo pipefail
 
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
-shift || true
+[ $# -ge 1 ] || { echo "usage: build_ref.sh REF_ROOT [DIMS ...]" >&2; exit 2; }
+REF="$1"
+shift
 DIMS=("$@")
 if [ ${#DIMS[@]} -eq 0 ]; then
     DIMS=(4x4x4x4 6x4x4x8 8x8x8x8 24x24x24x24 48x48x48x48)

@@ -64,6 +64,49 @@ def test_ape_without_allocation_matches_handle_path():
     ref.close()
 
 
+def test_ape_without_allocation_temporal_on_non_cubic_lattice():
+    """Temporal smearing on 6x4x4x8 (other strides, only the t links change): the handle path and the
+    reference's own smearing_APE_temporal output agree with the no-allocation entry point."""
+    lib = su2g.load()
+    g = O.golden()["lattices"]["6x4x4x8"]
+    spec = g["ape"]["temporal"]
+    dims, _, U = O.golden_config(g["base"])
+    _, _, want = O.golden_config(spec["cfg"])
+    cdims = (ctypes.c_int32 * 4)(*dims)
+    buf = DeviceBuffer(U.nbytes)
+    buf.upload(np.ascontiguousarray(U))
+    ref = Lattice(dims, precision="fp64")
+    ref.upload(U)
+    got = np.empty_like(U)
+    rc = lib.su2g_ape_inplace_noalloc(buf.ptr, cdims, spec["ns"], spec["alpha"], su2g.APE["temporal"], None)
+    assert rc == 0, lib.su2g_last_error(None)
+    ref.ape(spec["ns"], spec["alpha"], "temporal")
+    buf.download(got)
+    assert np.max(np.abs(got - ref.download())) <= 1e-13
+    assert np.max(np.abs(got - want)) <= 1e-13
+    buf.free()
+    ref.close()
+
+
+def test_ape_without_allocation_rejects_bad_pointers():
+    """A field pointer that is not 16-byte aligned, or not device memory, is refused before any launch."""
+    lib = su2g.load()
+    dims = (ctypes.c_int32 * 4)(4, 4, 4, 4)
+    nbytes = 4 ** 4 * 16 * 8
+    buf = DeviceBuffer(nbytes + 16)
+    off8 = ctypes.c_void_p(buf.ptr.value + 8)
+    assert lib.su2g_ape_inplace_noalloc(off8, dims, 1, 0.5, 0, None) == -1
+    assert b"not 16-byte aligned" in lib.su2g_last_error(None)
+    host = np.zeros(4 ** 4 * 16 + 2, dtype=np.float64)
+    hp = host.ctypes.data + (-host.ctypes.data) % 16
+    assert lib.su2g_ape_inplace_noalloc(ctypes.c_void_p(hp), dims, 1, 0.5, 0, None) == -1
+    assert b"not device memory" in lib.su2g_last_error(None)
+    # the device is still usable: a correct call on the aligned buffer goes through
+    assert lib.su2g_ape_inplace_noalloc(buf.ptr, dims, 0, 0.5, 0, None) == 0
+    assert buf.rt.cudaDeviceSynchronize() == 0
+    buf.free()
+
+
 def test_ape_without_allocation_rejects_oversized_lattice():
     lib = su2g.load()
     buf = DeviceBuffer(64)
