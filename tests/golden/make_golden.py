@@ -2,7 +2,7 @@
 """Generate the golden fixtures under tests/golden/ from the reference's own C code.
 
 This script is the provenance of every file next to it.  It needs the reference
-tree (default /root/reference, override with SU2_REFERENCE_ROOT) and gcc; it
+tree ($SU2_REFERENCE_ROOT, else a `reference` directory beside the repository) and gcc; it
 compiles the reference from its sources with oracle/build_ref.sh and runs the
 resulting harness binaries (oracle/ref_harness.c).  The GPU box has no
 reference tree, which is why the outputs are committed.
@@ -32,6 +32,17 @@ Outputs
                  AR(1) series, and Analysis/static potential/static_potential.py (run here,
                  its plotting module replaced by a no-op stand-in, matplotlib being absent) on
                  1000 configurations of W(R<=12, T<=20).  `make_golden.py --stats-only`.
+  golden.json["thesis_24x24x24x24_b3.09"]  equilibrium averages of the reference's own thesis
+                 chains at 24^4, beta 3.09 (one configuration per heatbath sweep, hot and cold
+                 starts), read from the WIL lines of its logs:
+                 measurements/Therm/24x24x24x24_SU2_b3.090000_id1_{hot,cold}_1.meas (unsmeared
+                 W(1,1), W(1,5), W(5,1), W(5,5); 4999 sweeps) and
+                 Thermalisation/24x24x24x24_SU2_b3.090000_id1_{hot,cold}_NAPE_100.meas (W(10,16)
+                 after 100 spatial APE steps; 10000 sweeps).  Per chain: the sweeps before
+                 `cut` dropped, the mean, the t_int.c Gamma-method error (tests/_stats.py) and a
+                 binned error (blocks of 100 sweeps); the test uses the larger.  The two starts
+                 are combined by inverse-variance weights, the error scaled by sqrt(chi^2/dof)
+                 where they disagree.  `make_golden.py --thesis-only`.
   kp_improved.dat  the reference's Kennedy-Pendleton sampler histogram at
                  alpha=7 (copied from LGT_Code/main_test/improved.dat; 200 bins
                  of N=1e8 draws; column 2 is count*200/N).
@@ -47,7 +58,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("SU2_REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("SU2_REFERENCE_ROOT") or os.path.join(os.path.dirname(REPO), "reference")
 
 LATTICES = {
     # dims T,X,Y,Z : (start, seed, beta, sweeps)
@@ -184,12 +195,83 @@ def stats_golden(gold):
     gold["stats"] = out
 
 
+# The thesis chains: which log, which loops, and where each start is thermalised.  The hot start's
+# W(5,5) and smeared W(10,16) still drift for thousands of sweeps (1000-sweep window means), so
+# the cuts are set where the window means of both starts have levelled off.
+THESIS = {
+    "unsmeared": {"file": "measurements/Therm/24x24x24x24_SU2_b3.090000_id1_%s_1.meas",
+                  "loops": [(1, 1), (1, 5), (5, 1), (5, 5)], "cut": {"hot": 2500, "cold": 2500}},
+    "ape_spatial_100": {"file": "Thermalisation/24x24x24x24_SU2_b3.090000_id1_%s_NAPE_100.meas",
+                        "loops": [(10, 16)], "cut": {"hot": 4000, "cold": 2500}},
+}
+THESIS_BLOCK = 100
+
+
+def _wil_lines(path):
+    """Per configuration, {(R, T): W} from the WIL lines of a meas log (meas.c:113)."""
+    import re
+    confs = []
+    for block in open(path).read().split("Measuring on configuration:")[1:]:
+        confs.append({(int(m.group(1)), int(m.group(2))): float(m.group(3))
+                      for m in re.finditer(r"WIL (\d+) (\d+)\s+(\S+)", block)})
+    return confs
+
+
+def binned_err(x, block):
+    x = np.asarray(x, dtype=np.float64)
+    nb = len(x) // block
+    m = x[: nb * block].reshape(nb, block).mean(axis=1)
+    return float(m.std(ddof=1) / np.sqrt(nb))
+
+
+def thesis_golden(gold):
+    sys.path.insert(0, os.path.dirname(HERE))
+    import _stats
+    out = {"dims": [24, 24, 24, 24], "beta": 3.09, "block": THESIS_BLOCK,
+           "note": "reference thesis chains, one configuration per heatbath sweep; error = max(Gamma method "
+                   "of t_int.c, binned); hot and cold starts combined by inverse-variance weights, the error scaled by "
+                   "sqrt(chi^2/dof) where they disagree",
+           "sets": {}}
+    for name, spec in THESIS.items():
+        obs = {}
+        for start in ("hot", "cold"):
+            rel = spec["file"] % start
+            confs = _wil_lines(os.path.join(REF, rel))
+            cut = spec["cut"][start]
+            for R, T in spec["loops"]:
+                x = np.array([c[(R, T)] for c in confs])[cut:]
+                m, eg, tau = _stats.mean_err(x)
+                eb = binned_err(x, THESIS_BLOCK)
+                obs.setdefault(f"{R},{T}", {"R": R, "T": T, "chains": {}})["chains"][start] = {
+                    "file": rel, "configurations": len(confs), "cut": cut, "mean": m, "err_gamma": eg,
+                    "tau_int": tau, "err_binned": eb, "err": max(eg, eb)}
+        for o in obs.values():
+            w = {k: 1.0 / c["err"] ** 2 for k, c in o["chains"].items()}
+            o["mean"] = sum(w[k] * c["mean"] for k, c in o["chains"].items()) / sum(w.values())
+            # where the two starts disagree by more than their errors, the error of the combination is
+            # scaled by sqrt(chi^2 / dof) (the scale factor of the Particle Data Group's averages)
+            chi2 = sum(w[k] * (c["mean"] - o["mean"]) ** 2 for k, c in o["chains"].items())
+            o["scale"] = float(max(1.0, np.sqrt(chi2 / (len(w) - 1))))
+            o["err"] = float(o["scale"] / np.sqrt(sum(w.values())))
+        out["sets"][name] = list(obs.values())
+    gold["thesis_24x24x24x24_b3.09"] = out
+
+
 def main():
     if "--stats-only" in sys.argv:
         path = os.path.join(HERE, "golden.json")
         with open(path) as f:
             gold = json.load(f)
         stats_golden(gold)
+        with open(path, "w") as f:
+            json.dump(gold, f, indent=1)
+        print("updated", path)
+        return 0
+    if "--thesis-only" in sys.argv:
+        path = os.path.join(HERE, "golden.json")
+        with open(path) as f:
+            gold = json.load(f)
+        thesis_golden(gold)
         with open(path, "w") as f:
             json.dump(gold, f, indent=1)
         print("updated", path)
@@ -296,6 +378,7 @@ def main():
     reflect_golden(gold)
     metro_golden(gold)
     stats_golden(gold)
+    thesis_golden(gold)
     shutil.copyfile(os.path.join(REF, "LGT_Code", "main_test", "improved.dat"), os.path.join(HERE, "kp_improved.dat"))
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(gold, f, indent=1)
