@@ -173,7 +173,12 @@ namespace {
 
 // ----------------------------------------------------------- sampler test ---
 
-// x0 histogram of the Kennedy-Pendleton sampler at fixed alpha (LGT_Code/main_test/test.c:115-166).
+// x0 histogram of the Kennedy-Pendleton sampler at fixed alpha (LGT_Code/main_test/test.c:115-166),
+// drawn by the production sampler heatbath_link<R> of the sweeps in the handle's precision: with the
+// staple A = 1 and beta = alpha it samples at alpha = |A| beta and returns X itself (A/|A| = 1), so
+// the FP32 histogram exercises the FP32 sampler's fast logarithm, sine/cosine, approximate square
+// roots and delta clamp.  Draw i uses the Philox stream of site i (sweep i >> 32, direction 0).
+template <typename R>
 __global__ void __launch_bounds__(kBlock) k_kp_histogram(double alpha, uint64_t seed, long long n, int nbins,
                                                          unsigned long long* __restrict__ counts,
                                                          unsigned* __restrict__ status)
@@ -181,27 +186,13 @@ __global__ void __launch_bounds__(kBlock) k_kp_histogram(double alpha, uint64_t 
     extern __shared__ unsigned int sh_hist[];
     for (int b = threadIdx.x; b < nbins; b += blockDim.x) sh_hist[b] = 0;
     __syncthreads();
-    const double ia = 1.0 / alpha;
+    const Q<R> A = q_one<R>();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        double delta = 0.0;
-        uint32_t trial = 0;
-        bool ok = false;
-        while (trial < kMaxTrials) {
-            U4 w = link_random(seed, (uint32_t)i, (uint32_t)(i >> 32), 0u, trial, 0u, kStreamUpdate, 0u);
-            ++trial;
-            const double c = cospi(2.0 * u01(w.z, 0.0));
-            delta = -(log(u01(w.y, 0.0)) + log(u01(w.x, 0.0)) * (c * c)) * ia;
-            const double u3 = u01(w.w, 0.0);
-            if (u3 * u3 <= 1.0 - 0.5 * delta) {
-                ok = true;
-                break;
-            }
-        }
-        if (!ok) {
-            atomicOr(status, kStatusKpTrials);
-            continue;
-        }
-        int b = (int)((2.0 - delta) * 0.5 * nbins);   // bin of x0 = 1 - delta on [-1, 1]
+        Q<R> X;
+        uint32_t trials = 0;
+        if (!heatbath_link<R>(A, (R)alpha, seed, (uint32_t)i, (uint32_t)(i >> 32), 0u, 0u, trials, X, status))
+            continue;   // trial bound hit: the status word tells the host
+        int b = (int)(((double)X.c0 + 1.0) * 0.5 * nbins);   // bin of x0 on [-1, 1]
         b = b < 0 ? 0 : (b >= nbins ? nbins - 1 : b);
         atomicAdd(&sh_hist[b], 1u);
     }
@@ -319,8 +310,12 @@ extern "C" int su2g_kp_histogram(su2g_lattice* h, double alpha, uint64_t seed, i
     if (!rc) {
         const int grid = grid_for(h, n, 8);
         launch_begin(h, SU2G_K_OTHER);
-        k_kp_histogram<<<grid, kBlock, nbins * sizeof(unsigned int), h->stream>>>(alpha, seed, n, nbins, d_counts,
-                                                                                 h->d_status);
+        if (h->prec == SU2G_FP32)
+            k_kp_histogram<float><<<grid, kBlock, nbins * sizeof(unsigned int), h->stream>>>(alpha, seed, n, nbins,
+                                                                                            d_counts, h->d_status);
+        else
+            k_kp_histogram<double><<<grid, kBlock, nbins * sizeof(unsigned int), h->stream>>>(alpha, seed, n, nbins,
+                                                                                             d_counts, h->d_status);
         rc = launch_end(h, SU2G_K_OTHER, "sampler histogram");
     }
     if (!rc)
