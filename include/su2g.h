@@ -212,6 +212,12 @@ int su2g_qtop(su2g_lattice *h, double *q, double *sum_abs);
  * between.  The handle's field is not modified.  The scratch (su2g_vjp_plan) comes from a memory
  * pool of the handle that keeps it for later calls until su2g_destroy. */
 int su2g_ape_qtop_vjp(su2g_lattice *h, int32_t n_ape, double alpha, int32_t ckpt, double *q, double *grad);
+/* One step along su(2) coefficients, the step an optimiser takes along the VJP's gradient (no
+ * counterpart in the reference): every link U -> exp(eps X) U with X = i x.sigma, x = three
+ * doubles per link in the gradient's layout double[V][4][3] (host memory), exp computed exactly
+ * (cos(eps|x|), sin(eps|x|) x/|x|).  With eps = +-e it is the perturbation of a central finite
+ * difference along x.  Synchronises. */
+int su2g_tangent_step(su2g_lattice *h, const double *x, double eps);
 /* Levels the VJP keeps on the device and its device memory, for a given n_ape and ckpt. */
 int su2g_vjp_plan(const su2g_lattice *h, int32_t n_ape, int32_t ckpt, int32_t *levels_stored,
                   int64_t *device_bytes);
@@ -237,7 +243,26 @@ const char *su2g_batch_last_error(const su2g_batch *b);
  * ms (may be NULL) receives the device time of the replays. */
 int su2g_batch_run(su2g_batch *b, int32_t n_sweeps, int32_t n_hb, int32_t n_or, int32_t meas_every,
                    double *plaq_trace, double *ms);
-/* Times the sweep for each candidate CTA size and keeps the fastest (the fields are restored). */
+/* How a batch runs its sweeps.  SU2G_BATCH_GRAPH: one launch per checkerboard pass for all replicas
+ * (CTAs mapped to replicas by the replica-offset table), a measurement block captured once in a CUDA
+ * graph and replayed.  SU2G_BATCH_PERSISTENT: the whole su2g_batch_run as one cooperative launch
+ * whose resident CTAs walk every pass as one global link index over all replicas (small replicas
+ * share a CTA) and meet at a bounded grid-wide barrier between passes; a barrier that waits too
+ * long makes the run return SU2G_EDEVICE.  Both draw the same Philox streams: results are
+ * identical. */
+enum su2g_batch_mode { SU2G_BATCH_GRAPH = 0, SU2G_BATCH_PERSISTENT = 1 };
+/* Choose the form and the CTA width (64, 128 or 256 threads; 128 or 256 for the persistent form). */
+int su2g_batch_configure(su2g_batch *b, int32_t mode, int32_t block);
+int su2g_batch_config(const su2g_batch *b, int32_t *mode, int32_t *block);
+/* Diagnostic of the persistent form's bounded grid-wide barrier (no counterpart in the reference):
+ * one cooperative launch of one CTA per SM passes two barriers that wait for `missing` more CTAs
+ * than the grid holds.  missing = 0 returns SU2G_OK; missing > 0 lets every CTA give up after
+ * wait_cycles SM clock cycles, and the call returns SU2G_EDEVICE with the reason -- without a fault,
+ * the batch staying usable. */
+int su2g_batch_selftest_grid_barrier(su2g_batch *b, int32_t missing, int64_t wait_cycles);
+/* Times both forms over their CTA widths (sweeps of n_hb + n_or with a plaquette after each) and
+ * keeps the fastest, returning its CTA width in block_out (su2g_batch_config gives the form); the
+ * fields and counters are restored. */
 int su2g_batch_autotune(su2g_batch *b, int32_t n_hb, int32_t n_or, int32_t *block_out);
 /* The integrated autocorrelation analysis of LGT_Code/Autocorrelation/t_int.c (see
  * su2g_stats_tau_int) of every replica's plaquette trace from the last su2g_batch_run, on the
@@ -249,7 +274,9 @@ int su2g_batch_upload(su2g_batch *b, int32_t r, const double *links);
 
 /* ---- Kennedy-Pendleton sampler alone (generateSU2InHeatbath_Improved, heatbath.c:76-121;
  * the reference's sampler test LGT_Code/main_test/test.c:115-166): counts of x0 in nbins
- * equal bins on [-1,1] for n draws at fixed alpha. */
+ * equal bins on [-1,1] for n draws at fixed alpha, drawn by the same per-link sampler the
+ * heatbath sweeps run, in the handle's precision (FP32: fast logarithm and sine/cosine,
+ * approximate square roots, delta clamped at 0). */
 int su2g_kp_histogram(su2g_lattice *h, double alpha, uint64_t seed, int64_t n, int32_t nbins,
                       int64_t *counts);
 
@@ -261,9 +288,11 @@ int su2g_kp_histogram(su2g_lattice *h, double alpha, uint64_t seed, int64_t n, i
  * ns steps of `mode` with parameter alpha, enqueued on cuda_stream (NULL = default stream); the
  * call does not synchronise.  The intermediate level lives in a static device array of 48 MiB
  * that every GPU loading the library keeps until exit; lattices above 393216 sites are rejected
- * with SU2G_EINVAL.  The first call on a device looks up that array's address (issue it before
- * any stream capture).  All calls share the array: calls that overlap on the GPU race.  Errors
- * are reported by su2g_last_error(NULL). */
+ * with SU2G_EINVAL, and so is a field pointer that is not 16-byte aligned device (or managed)
+ * memory of the current device.  The first call on a device looks up that array's address (issue
+ * it before any stream capture); the address is cached for the life of the process, so after
+ * cudaDeviceReset this entry point must not be called again in that process.  All calls share the
+ * array: calls that overlap on the GPU race.  Errors are reported by su2g_last_error(NULL). */
 int su2g_ape_inplace_noalloc(double *links, const int32_t dims[4], int32_t ns, double alpha, int32_t mode,
                              void *cuda_stream);
 

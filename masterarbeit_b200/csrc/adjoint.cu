@@ -435,6 +435,30 @@ int segment_length(int n_ape, int ckpt)
     return std::max(c, 1);
 }
 
+// One step along su(2) coefficients x (per site and direction, the layout of the VJP's gradient):
+// U_mu(n) <- exp(eps X) U_mu(n), X = i x.sigma, exp(eps X) = (cos(eps|x|), sin(eps|x|) x/|x|), for
+// the sites [n0, n0 + count) whose coefficients are in `xs` (12 doubles per site).
+template <typename R>
+__global__ void __launch_bounds__(kBlock) k_tangent_step(const double* __restrict__ xs, Field<R> U, Geom g, int n0,
+                                                         int count, double eps)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const int n = n0 + i;
+        int par;
+        const Site s = site_lex(g, n, par);
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) {
+            const double* x = xs + (size_t)i * 12 + 3 * mu;
+            const double nx = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+            double sn, cs;
+            sincos(eps * nx, &sn, &cs);
+            const double f = nx > 0.0 ? sn / nx : 0.0;
+            const Q<R> E = q_make<R>((R)cs, (R)(f * x[0]), (R)(f * x[1]), (R)(f * x[2]));
+            U.sth(mu, par, n >> 1, q_mul(E, U.ld(mu, par, s.n)));
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" int su2g_ape_qtop_vjp(su2g_lattice* h, int32_t n_ape, double alpha, int32_t ckpt, double* q, double* grad)
@@ -461,4 +485,30 @@ extern "C" int su2g_vjp_plan(const su2g_lattice* h, int32_t n_ape, int32_t ckpt,
     if (device_bytes)
         *device_bytes = (int64_t)(levels + 5) * field + 6ll * h->g.V * (int64_t)h->link_bytes + 96ll * h->g.V;
     return SU2G_OK;
+}
+
+extern "C" int su2g_tangent_step(su2g_lattice* h, const double* x, double eps)
+{
+    if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_tangent_step: null handle");
+    if (!x || !std::isfinite(eps)) return set_error(h, SU2G_EINVAL, "su2g_tangent_step: bad argument");
+    cudaSetDevice(h->device);
+    int rc = ensure_aos(h);   // the coefficients stream through the transfer staging, 12 of its 16 doubles a site
+    if (rc) return rc;
+    for (size_t n0 = 0; n0 < (size_t)h->g.V; n0 += h->aos_sites) {
+        const int cnt = (int)std::min(h->aos_sites, (size_t)h->g.V - n0);
+        rc = check_cuda(h, cudaMemcpyAsync(h->d_aos, x + n0 * 12, (size_t)cnt * 12 * sizeof(double),
+                                           cudaMemcpyHostToDevice, h->stream),
+                        "uploading tangent coefficients");
+        if (rc) return rc;
+        const int grid = grid_for(h, cnt, 8);
+        launch_begin(h, SU2G_K_OTHER);
+        if (h->prec == SU2G_FP32)
+            k_tangent_step<float><<<grid, kBlock, 0, h->stream>>>(h->d_aos, make_field<float>(h->dirp, h->g.Vh), h->g,
+                                                                 (int)n0, cnt, eps);
+        else
+            k_tangent_step<double><<<grid, kBlock, 0, h->stream>>>(h->d_aos, make_field<double>(h->dirp, h->g.Vh), h->g,
+                                                                  (int)n0, cnt, eps);
+        if ((rc = launch_end(h, SU2G_K_OTHER, "tangent step"))) return rc;
+    }
+    return check_cuda(h, cudaStreamSynchronize(h->stream), "tangent step");
 }

@@ -9,6 +9,13 @@
 // replayed; the Philox sweep index and the measurement slot live in device counters that the graph
 // advances itself.  Each replica draws the same Philox streams as a single-lattice handle with the
 // same (seed, replica id), so a batch and a set of single handles give identical fields.
+//
+// Persistent form.  Alternatively one cooperative launch runs every measurement block of a
+// su2g_batch_run: its CTAs (all resident) walk the links of each pass as one global index over all
+// replicas, in tiles of one CTA's width, so small replicas share a CTA, and meet at a grid-wide
+// barrier between passes.  The barrier's wait is bounded: a CTA that waits too long raises
+// kStatusGridTimeout and every CTA leaves at its next barrier.  su2g_batch_autotune times both
+// forms over CTA widths and keeps the fastest.
 #include <algorithm>
 #include <cmath>
 #include <new>
@@ -33,6 +40,11 @@ struct Replica {
 
 enum { kCtrSweep = 0, kCtrMeas = 1 };
 
+// Grid-wide barrier state of the persistent form (zeroed before every launch).
+struct GridBarrier {
+    unsigned count, gen, abort, pad;
+};
+
 }  // namespace
 
 struct su2g_batch {
@@ -53,6 +65,9 @@ struct su2g_batch {
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int g_hb = -1, g_or = -1, g_meas = -1, g_every = -1, g_block = -1;
+    int mode = SU2G_BATCH_GRAPH;                   // su2g_batch_mode
+    int* d_upre = nullptr;                         // first global link index of each replica in a pass (n+1)
+    GridBarrier* d_gb = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     char err[512] = {0};
 };
@@ -220,6 +235,190 @@ __global__ void __launch_bounds__(256) k_batch_aos(const Replica* __restrict__ r
     }
 }
 
+// ---------------------------------------------------------------- persistent form ---
+
+constexpr long long kGridWaitCycles = 4000000000ll;   // about 2 s at the B200's clock
+
+// Grid-wide barrier of a cooperative launch (every CTA resident).  Thread 0 of each CTA arrives on
+// a counter; the last of `arrivals` (default: every CTA) resets it and advances the generation the
+// others poll.  The poll gives up
+// after kGridWaitCycles or when another CTA has given up; then the CTA raises kStatusGridTimeout and
+// every CTA returns false here, now or at its next barrier, so none is left waiting.  The fences
+// make the field writes of the pass before the barrier visible to the loads after it.
+__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned* status, unsigned arrivals = 0u,
+                                          long long wait_cycles = kGridWaitCycles)
+{
+    if (arrivals == 0u) arrivals = gridDim.x;
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = &gb->gen;
+        volatile unsigned* vabort = &gb->abort;
+        const unsigned g0 = *vgen;
+        int ok = 1;
+        __threadfence();
+        if (atomicAdd(&gb->count, 1u) == arrivals - 1) {
+            atomicExch(&gb->count, 0u);
+            __threadfence();
+            atomicAdd(&gb->gen, 1u);
+        } else {
+            const long long t0 = clock64();
+            while (*vgen == g0) {
+                if (*vabort || clock64() - t0 > wait_cycles) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        if (!ok) {
+            atomicExch(&gb->abort, 1u);
+            atomicOr(status, kStatusGridTimeout);
+        }
+        __threadfence();
+        s_ok = ok && !*vabort;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+struct PersistArgs {
+    const Replica* reps;
+    const int* upre;     // n+1 first global link index of each replica in a pass
+    const int* smap;     // site chunk -> replica, chunks of blockDim sites (the plaquette)
+    const int* sblk;     // n+1 first site chunk of each replica
+    int n, nblocks, every, n_hb, n_or, meas;
+    uint32_t* ctr;
+    double* trace;
+    DD* partials;
+    GridBarrier* gb;
+    unsigned* status;
+};
+
+template <typename R>
+__device__ __forceinline__ FieldCG<R> rep_field_cg(const Replica& r)
+{
+    FieldCG<R> f;
+    for (int mu = 0; mu < 4; ++mu) f.p[mu] = reinterpret_cast<typename Field<R>::ptr_t>(r.dirs[mu]);
+    f.Vh = r.g.Vh;
+    return f;
+}
+
+// One checkerboard pass (mu, par) over every replica: global link index gi over all replicas, tiles
+// of one CTA's width, tile k handled by CTA k mod gridDim (in order, so the CTAs in flight cover a
+// contiguous window of the pool).  The link of gi is h = gi - upre[r] of the replica r with
+// upre[r] <= gi < upre[r+1] (binary search in shared memory).
+template <typename R, int MU, int KIND>
+__device__ __forceinline__ void persist_pass(const PersistArgs& a, const int* __restrict__ s_pre, int par,
+                                             uint32_t sweep)
+{
+    const int total = s_pre[a.n];
+    for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < total; gi += gridDim.x * blockDim.x) {
+        int lo = 0, hi = a.n;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_pre[mid] <= gi) lo = mid;
+            else hi = mid;
+        }
+        const Replica& rp = a.reps[lo];
+        const Geom g = rp.g;
+        const int h = gi - s_pre[lo];
+        const FieldCG<R> U = rep_field_cg<R>(rp);
+        const Site s = site_of(g, par, h);
+        const Q<R> A = staple_update<R, MU, FieldCG<R>>(U, g, s, par);
+        if (KIND == SU2G_HEATBATH) {
+            Q<R> out;
+            uint32_t trials = 0;
+            if (heatbath_link<R>(A, (R)rp.beta, rp.seed, (uint32_t)s.n, sweep, (uint32_t)MU, rp.id, trials, out,
+                                 a.status))
+                U.sth(MU, par, h, q_project(out));
+        } else {
+            U.sth(MU, par, h, q_project(overrelax_link<R>(A, U.ldh(MU, par, h))));
+        }
+    }
+}
+
+template <typename R, int KIND>
+__device__ __forceinline__ void persist_pass_mu(const PersistArgs& a, const int* s_pre, int mu, int par, uint32_t sweep)
+{
+    switch (mu) {
+        case 0: persist_pass<R, 0, KIND>(a, s_pre, par, sweep); break;
+        case 1: persist_pass<R, 1, KIND>(a, s_pre, par, sweep); break;
+        case 2: persist_pass<R, 2, KIND>(a, s_pre, par, sweep); break;
+        default: persist_pass<R, 3, KIND>(a, s_pre, par, sweep); break;
+    }
+}
+
+// Every measurement block of a run in one launch: `every` sweeps of n_hb heatbath and n_or
+// overrelaxation passes, then (if meas) each replica's plaquette into its trace slot, exactly the
+// work and the Philox streams of the replayed graph of launches.
+template <typename R, int NT>
+__global__ void __launch_bounds__(NT, (sizeof(R) == 8 ? 512 : 1024) / NT) k_batch_persist(PersistArgs a)
+{
+    extern __shared__ int s_pre[];
+    for (int i = threadIdx.x; i <= a.n; i += NT) s_pre[i] = a.upre[i];
+    __syncthreads();
+    // every CTA reads the counters here; CTA 0 writes them back only after the last barrier
+    uint32_t sweep = a.ctr[kCtrSweep], slot = a.ctr[kCtrMeas];
+    const int nchunks = a.sblk[a.n];
+    for (int blk = 0; blk < a.nblocks; ++blk) {
+        for (int s = 0; s < a.every; ++s) {
+            for (int i = 0; i < a.n_hb; ++i, ++sweep)
+                for (int mu = 0; mu < 4; ++mu)
+                    for (int par = 0; par < 2; ++par) {
+                        persist_pass_mu<R, SU2G_HEATBATH>(a, s_pre, mu, par, sweep);
+                        if (!grid_sync(a.gb, a.status)) return;
+                    }
+            for (int i = 0; i < a.n_or; ++i)
+                for (int mu = 0; mu < 4; ++mu)
+                    for (int par = 0; par < 2; ++par) {
+                        persist_pass_mu<R, SU2G_OVERRELAX>(a, s_pre, mu, par, 0u);
+                        if (!grid_sync(a.gb, a.status)) return;
+                    }
+        }
+        if (!a.meas) continue;
+        // plaquette partials: site chunk c of replica r covers sites (c - sblk[r]) NT .. + NT - 1
+        for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+            const int r = a.smap[c];
+            const Replica& rp = a.reps[r];
+            const Geom g = rp.g;
+            const int i = (c - a.sblk[r]) * NT + threadIdx.x;
+            double site = 0.0;
+            if (i < g.V) {
+                const FieldCG<R> U = rep_field_cg<R>(rp);
+                int par;
+                const Site st = site_lex(g, i, par);
+                const int h = i >> 1, q = par ^ 1;
+#pragma unroll
+                for (int mu = 0; mu < 3; ++mu)
+#pragma unroll
+                    for (int nu = mu + 1; nu < 4; ++nu) {
+                        const Q<R> x = q_mul(U.ldh(mu, par, h), U.ld(nu, q, st.n + up_off_rt(g, st.c, mu)));
+                        const Q<R> y = q_mul(U.ldh(nu, par, h), U.ld(mu, q, st.n + up_off_rt(g, st.c, nu)));
+                        site += (double)q_dot(x, y);
+                    }
+            }
+            const DD v = dd_block_sum<NT>(DD{site, 0.0});
+            if (threadIdx.x == 0) a.partials[c] = v;
+        }
+        if (!grid_sync(a.gb, a.status)) return;
+        // one CTA per replica: fixed-order sum of its chunks' partials
+        for (int r = blockIdx.x; r < a.n; r += gridDim.x) {
+            DD acc = {0.0, 0.0};
+            for (int c = a.sblk[r] + threadIdx.x; c < a.sblk[r + 1]; c += NT)
+                acc = dd_add(acc, DD{__ldcg(&a.partials[c].s), __ldcg(&a.partials[c].e)});
+            acc = dd_block_sum<NT>(acc);
+            if (threadIdx.x == 0) a.trace[(size_t)slot * a.n + r] = (acc.s + acc.e) / (6.0 * (double)a.reps[r].g.V);
+        }
+        ++slot;
+        if (!grid_sync(a.gb, a.status)) return;   // the partials are written again by the next block
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.ctr[kCtrSweep] = sweep;
+        a.ctr[kCtrMeas] = slot;
+    }
+}
+
 // CTA maps for a block size: CTAs of replica r are [blk[r], blk[r+1]).
 int build_maps(su2g_batch* b, int block)
 {
@@ -316,12 +515,68 @@ int ensure_graph(su2g_batch* b, int n_hb, int n_or, int every, int meas)
     return SU2G_OK;
 }
 
+// Diagnostic of the bounded barrier: two barriers that wait for `arrivals` CTAs.  With one arrival
+// more than the grid has, nobody is last, every CTA gives up after wait_cycles and the status word
+// says so; nothing faults and no CTA is left waiting.
+__global__ void __launch_bounds__(128) k_grid_selftest(GridBarrier* gb, unsigned* status, unsigned arrivals,
+                                                       long long wait_cycles)
+{
+    if (!grid_sync(gb, status, arrivals, wait_cycles)) return;
+    grid_sync(gb, status, arrivals, wait_cycles);
+}
+
+template <typename R, int NT>
+int launch_persist_t(su2g_batch* b, const PersistArgs& a)
+{
+    const size_t smem = (size_t)(b->n + 1) * sizeof(int);
+    int per_sm = 0;
+    int rc = bcuda(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persist<R, NT>, NT, smem),
+                   "occupancy of the persistent sweep");
+    if (rc) return rc;
+    if (per_sm < 1) return berr(b, SU2G_ECUDA, "the persistent sweep kernel does not fit on an SM");
+    const int grid = b->num_sms * per_sm;   // all resident: the cooperative launch checks it
+    PersistArgs args = a;
+    void* params[] = {&args};
+    return bcuda(b, cudaLaunchCooperativeKernel((const void*)k_batch_persist<R, NT>, dim3(grid), dim3(NT), params, smem,
+                                                b->stream),
+                 "launching the persistent sweep");
+}
+
+// Every block of a run as one cooperative launch (the persistent form).
+int launch_persist(su2g_batch* b, int nblocks, int n_hb, int n_or, int every, int meas)
+{
+    PersistArgs a;
+    a.reps = b->d_reps;
+    a.upre = b->d_upre;
+    a.smap = b->d_smap;
+    a.sblk = sblk0(b);
+    a.n = b->n;
+    a.nblocks = nblocks;
+    a.every = every;
+    a.n_hb = n_hb;
+    a.n_or = n_or;
+    a.meas = meas;
+    a.ctr = b->d_ctr;
+    a.trace = b->d_trace;
+    a.partials = b->partials;
+    a.gb = b->d_gb;
+    a.status = b->d_status;
+    int rc = bcuda(b, cudaMemsetAsync(b->d_gb, 0, sizeof(GridBarrier), b->stream), "clearing the grid barrier");
+    if (rc) return rc;
+    if (b->block == 128)
+        return b->prec == SU2G_FP32 ? launch_persist_t<float, 128>(b, a) : launch_persist_t<double, 128>(b, a);
+    return b->prec == SU2G_FP32 ? launch_persist_t<float, 256>(b, a) : launch_persist_t<double, 256>(b, a);
+}
+
 int check_status(su2g_batch* b)
 {
     unsigned st = 0;
     int rc = bcuda(b, cudaMemcpy(&st, b->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost), "reading status");
     if (rc) return rc;
+    if (st) cudaMemset(b->d_status, 0, sizeof(unsigned));   // reported once; the batch stays usable
     if (st & kStatusKpTrials) return berr(b, SU2G_EDEVICE, "a heatbath link exceeded %u Kennedy-Pendleton trials", kMaxTrials);
+    if (st & kStatusGridTimeout)
+        return berr(b, SU2G_EDEVICE, "the persistent sweep gave up waiting at a grid-wide barrier (the fields are not valid)");
     if (st) return berr(b, SU2G_EDEVICE, "device status word 0x%x", st);
     return SU2G_OK;
 }
@@ -344,6 +599,8 @@ extern "C" int su2g_batch_destroy(su2g_batch* b)
     cudaFree(b->d_ctr);
     cudaFree(b->d_status);
     cudaFree(b->d_trace);
+    cudaFree(b->d_upre);
+    cudaFree(b->d_gb);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -410,6 +667,19 @@ extern "C" int su2g_batch_create(const su2g_replica* reps, int32_t n, int32_t pr
                 b->reps[r].dirs[mu] = (char*)b->pool + off[r] + (size_t)mu * 2 * b->reps[r].g.Vh * b->link_bytes;
     if (!rc) rc = bcuda(b, cudaMalloc(&b->d_reps, n * sizeof(Replica)), "allocating the replica table");
     if (!rc) rc = bcuda(b, cudaMemcpy(b->d_reps, b->reps.data(), n * sizeof(Replica), cudaMemcpyHostToDevice), "table");
+    if (!rc) {
+        std::vector<int> upre(n + 1, 0);
+        long long tot = 0;
+        for (int r = 0; r < n; ++r) {
+            upre[r] = (int)tot;
+            tot += b->reps[r].g.Vh;
+        }
+        if (tot > (1ll << 30)) rc = berr(b, SU2G_EINVAL, "the replicas hold more than 2^31 links");
+        upre[n] = (int)tot;
+        if (!rc) rc = bcuda(b, cudaMalloc(&b->d_upre, (n + 1) * sizeof(int)), "allocating the link prefix table");
+        if (!rc) rc = bcuda(b, cudaMemcpy(b->d_upre, upre.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice), "table");
+        if (!rc) rc = bcuda(b, cudaMalloc(&b->d_gb, sizeof(GridBarrier)), "allocating the grid barrier");
+    }
     if (!rc) rc = bcuda(b, cudaMalloc(&b->d_ctr, 2 * sizeof(uint32_t)), "allocating counters");
     if (!rc) rc = bcuda(b, cudaMemset(b->d_ctr, 0, 2 * sizeof(uint32_t)), "clearing counters");
     if (!rc) rc = bcuda(b, cudaMalloc(&b->d_status, sizeof(unsigned)), "allocating status");
@@ -457,15 +727,20 @@ extern "C" int su2g_batch_run(su2g_batch* b, int32_t n_sweeps, int32_t n_hb, int
         if ((rc = bcuda(b, cudaMalloc(&b->d_trace, b->n * sizeof(double)), "allocating the trace"))) return rc;
         b->trace_cap = b->n;
     }
-    if ((rc = ensure_graph(b, n_hb, n_or, every, meas))) return rc;
+    const bool persist = b->mode == SU2G_BATCH_PERSISTENT;
+    if (!persist && (rc = ensure_graph(b, n_hb, n_or, every, meas))) return rc;
     // measurement slots restart at 0 for every run
     uint32_t zero = 0;
     if ((rc = bcuda(b, cudaMemcpyAsync(b->d_ctr + kCtrMeas, &zero, sizeof(zero), cudaMemcpyHostToDevice, b->stream),
                     "resetting the slot counter")))
         return rc;
     cudaEventRecord(b->ev0, b->stream);
-    for (int i = 0; i < nblocks; ++i)
-        if ((rc = bcuda(b, cudaGraphLaunch(b->graph, b->stream), "launching the sweep graph"))) return rc;
+    if (persist) {
+        if (nblocks > 0 && (rc = launch_persist(b, nblocks, n_hb, n_or, every, meas))) return rc;
+    } else {
+        for (int i = 0; i < nblocks; ++i)
+            if ((rc = bcuda(b, cudaGraphLaunch(b->graph, b->stream), "launching the sweep graph"))) return rc;
+    }
     cudaEventRecord(b->ev1, b->stream);
     if ((rc = bcuda(b, cudaStreamSynchronize(b->stream), "running sweeps"))) return rc;
     if (ms) {
@@ -519,20 +794,26 @@ extern "C" int su2g_batch_autotune(su2g_batch* b, int32_t n_hb, int32_t n_or, in
     int rc = bcuda(b, cudaMalloc(&save, pool_bytes), "allocating the autotune copy");
     if (!rc) rc = bcuda(b, cudaMemcpy(save, b->pool, pool_bytes, cudaMemcpyDeviceToDevice), "saving replicas");
     if (!rc) rc = bcuda(b, cudaMemcpy(ctr, b->d_ctr, sizeof(ctr), cudaMemcpyDeviceToHost), "saving counters");
-    const int candidates[] = {64, 128, 256};
+    // the two forms (replayed graph of per-pass launches; one persistent launch) over CTA widths,
+    // each timed on 4 sweeps with a plaquette after every sweep, after 2 warm-up sweeps
+    const int candidates[][2] = {{SU2G_BATCH_GRAPH, 64},       {SU2G_BATCH_GRAPH, 128}, {SU2G_BATCH_GRAPH, 256},
+                                 {SU2G_BATCH_PERSISTENT, 128}, {SU2G_BATCH_PERSISTENT, 256}};
     double best = 1e30;
-    int best_block = b->block;
-    for (int cb : candidates) {
+    int best_block = b->block, best_mode = b->mode;
+    for (const auto& c : candidates) {
         if (rc) break;
-        if ((rc = build_maps(b, cb))) break;
+        if ((rc = build_maps(b, c[1]))) break;
+        b->mode = c[0];
         double ms = 0;
-        if ((rc = su2g_batch_run(b, 2, n_hb, n_or, 0, nullptr, &ms))) break;   // warm-up + graph build
-        if ((rc = su2g_batch_run(b, 4, n_hb, n_or, 0, nullptr, &ms))) break;
+        if ((rc = su2g_batch_run(b, 2, n_hb, n_or, 1, nullptr, &ms))) break;   // warm-up + graph build
+        if ((rc = su2g_batch_run(b, 4, n_hb, n_or, 1, nullptr, &ms))) break;
         if (ms < best) {
             best = ms;
-            best_block = cb;
+            best_block = c[1];
+            best_mode = c[0];
         }
     }
+    b->mode = best_mode;
     if (!rc) rc = build_maps(b, best_block);
     if (!rc) rc = bcuda(b, cudaMemcpy(b->pool, save, pool_bytes, cudaMemcpyDeviceToDevice), "restoring replicas");
     if (!rc) rc = bcuda(b, cudaMemcpy(b->d_ctr, ctr, sizeof(ctr), cudaMemcpyHostToDevice), "restoring counters");
@@ -575,5 +856,48 @@ extern "C" int su2g_batch_upload(su2g_batch* b, int32_t r, const double* links)
     }
     if (!rc) rc = bcuda(b, cudaStreamSynchronize(b->stream), "uploading");
     cudaFree(d);
+    return rc;
+}
+
+extern "C" int su2g_batch_configure(su2g_batch* b, int32_t mode, int32_t block)
+{
+    if (!b) return set_error(nullptr, SU2G_EINVAL, "su2g_batch_configure: null batch");
+    if (mode != SU2G_BATCH_GRAPH && mode != SU2G_BATCH_PERSISTENT)
+        return berr(b, SU2G_EINVAL, "su2g_batch_configure: unknown mode %d", mode);
+    if (block != 64 && block != 128 && block != 256)
+        return berr(b, SU2G_EINVAL, "su2g_batch_configure: CTA width %d (64, 128 or 256)", block);
+    if (mode == SU2G_BATCH_PERSISTENT && block == 64)
+        return berr(b, SU2G_EINVAL, "su2g_batch_configure: the persistent form runs 128 or 256 threads a CTA");
+    cudaSetDevice(b->device);
+    b->mode = mode;
+    return block == b->block ? SU2G_OK : build_maps(b, block);
+}
+
+extern "C" int su2g_batch_config(const su2g_batch* b, int32_t* mode, int32_t* block)
+{
+    if (!b) return set_error(nullptr, SU2G_EINVAL, "su2g_batch_config: null batch");
+    if (mode) *mode = b->mode;
+    if (block) *block = b->block;
+    return SU2G_OK;
+}
+
+extern "C" int su2g_batch_selftest_grid_barrier(su2g_batch* b, int32_t missing, int64_t wait_cycles)
+{
+    if (!b) return set_error(nullptr, SU2G_EINVAL, "su2g_batch_selftest_grid_barrier: null batch");
+    if (missing < 0 || wait_cycles <= 0 || wait_cycles > kGridWaitCycles)
+        return berr(b, SU2G_EINVAL, "su2g_batch_selftest_grid_barrier: bad argument");
+    cudaSetDevice(b->device);
+    GridBarrier* gb = b->d_gb;
+    unsigned* st = b->d_status;
+    unsigned arrivals = (unsigned)(b->num_sms + missing);
+    long long wc = (long long)wait_cycles;
+    void* params[] = {&gb, &st, &arrivals, &wc};
+    int rc = bcuda(b, cudaMemsetAsync(b->d_gb, 0, sizeof(GridBarrier), b->stream), "clearing the grid barrier");
+    if (!rc)
+        rc = bcuda(b, cudaLaunchCooperativeKernel((const void*)k_grid_selftest, dim3(b->num_sms), dim3(128), params, 0,
+                                                  b->stream),
+                   "launching the barrier self-test");
+    if (!rc) rc = bcuda(b, cudaStreamSynchronize(b->stream), "barrier self-test");
+    if (!rc) rc = check_status(b);
     return rc;
 }

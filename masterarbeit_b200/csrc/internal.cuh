@@ -17,7 +17,7 @@ constexpr int kOutSlots = 16384;       // device result doubles per handle
 constexpr uint32_t kMaxTrials = 1u << 20;   // Kennedy-Pendleton trials before a link gives up
 
 // Status bits a kernel may raise in the handle's status word.
-enum : unsigned { kStatusKpTrials = 1u, kStatusNonFinite = 2u, kStatusTmaTimeout = 4u };
+enum : unsigned { kStatusKpTrials = 1u, kStatusNonFinite = 2u, kStatusTmaTimeout = 4u, kStatusGridTimeout = 8u };
 
 // Compensated sum: value s plus running error e (TwoSum, Knuth TAOCP vol. 2, 4.2.2).
 struct DD {

@@ -335,6 +335,33 @@ struct Field<double> {
     }
 };
 
+// The same views with loads through L2 only (ld.global.cg), for a kernel that reads links other
+// CTAs of the same launch have written (a persistent kernel, after a grid-wide barrier): the
+// read-only path of __ldg may serve such a link from a stale line.
+template <typename R>
+struct FieldCG;
+
+template <>
+struct FieldCG<float> : Field<float> {
+    __device__ __forceinline__ Q<float> ld(int mu, int par, int n) const { return ldh(mu, par, (int)((unsigned)n >> 1)); }
+    __device__ __forceinline__ Q<float> ldh(int mu, int par, int h) const
+    {
+        float4 v = __ldcg(p[mu] + (unsigned)(par * Vh + h));
+        return q_make<float>(v.x, v.y, v.z, v.w);
+    }
+};
+
+template <>
+struct FieldCG<double> : Field<double> {
+    __device__ __forceinline__ Q<double> ld(int mu, int par, int n) const { return ldh(mu, par, (int)((unsigned)n >> 1)); }
+    __device__ __forceinline__ Q<double> ldh(int mu, int par, int h) const
+    {
+        const double2* a = p[mu] + 2u * (unsigned)(par * Vh + h);
+        double2 x = __ldcg(a), y = __ldcg(a + 1);
+        return q_make<double>(x.x, x.y, y.x, y.y);
+    }
+};
+
 // Field view over four direction base pointers (each 2*Vh links long).
 template <typename R>
 inline Field<R> make_field(void* const dirs[4], int Vh)

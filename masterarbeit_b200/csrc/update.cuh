@@ -64,8 +64,8 @@ __device__ __forceinline__ double kp_clamp(double d) { return d; }
 //   A = sum_{nu != mu} U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag + U_nu(x-nu+mu)^dag U_mu(x-nu)^dag U_nu(x-nu)
 // All 18 links are loaded before the first product, so that a thread keeps every load of its
 // staple in flight at once (the pass is bound by memory latency x parallelism, not by ALU).
-template <typename R, int MU>
-__device__ __forceinline__ Q<R> staple_update(const Field<R>& U, const Geom& g, const Site& s, int par)
+template <typename R, int MU, typename F = Field<R>>
+__device__ __forceinline__ Q<R> staple_update(const F& U, const Geom& g, const Site& s, int par)
 {
     const int q = par ^ 1;
     const int dmu = up_off<MU>(g, s);

@@ -106,6 +106,7 @@ _SIGS = {
     "su2g_qtop": (ctypes.c_int, [_P, _DP, _DP]),
     "su2g_ape_qtop_vjp": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _DP, _DP]),
     "su2g_vjp_plan": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _I32P, _I64P]),
+    "su2g_tangent_step": (ctypes.c_int, [_P, _DP, ctypes.c_double]),
     "su2g_kp_histogram":(ctypes.c_int, [_P, ctypes.c_double, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32, _I64P]),
     "su2g_ape_inplace_noalloc": (ctypes.c_int, [_P, _I32P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _P]),
     "su2g_batch_create": (ctypes.c_int, [ctypes.POINTER(ReplicaSpec), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
@@ -114,6 +115,9 @@ _SIGS = {
     "su2g_batch_last_error": (ctypes.c_char_p, [_P]),
     "su2g_batch_run": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]),
     "su2g_batch_autotune": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _I32P]),
+    "su2g_batch_configure": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
+    "su2g_batch_config": (ctypes.c_int, [_P, _I32P, _I32P]),
+    "su2g_batch_selftest_grid_barrier": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int64]),
     "su2g_batch_download": (ctypes.c_int, [_P, ctypes.c_int32, _DP]),
     "su2g_batch_upload": (ctypes.c_int, [_P, ctypes.c_int32, _DP]),
     "su2g_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_P)]),
@@ -358,6 +362,13 @@ class Lattice:
                                                _as_dp(g) if grad else None))
         return (q.value, g) if grad else q.value
 
+    def tangent_step(self, x, eps):
+        """U -> exp(eps X) U for every link, x = su(2) coefficients in the gradient's layout (V, 4, 3)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.size != 12 * self.info()["volume"]:
+            raise ValueError("tangent coefficients must have V x 4 x 3 entries")
+        self._check(self.lib.su2g_tangent_step(self.h, x.ctypes.data_as(_DP), float(eps)))
+
     def vjp_plan(self, n_ape, ckpt=0):
         lev, nb = ctypes.c_int32(), ctypes.c_int64()
         self._check(self.lib.su2g_vjp_plan(self.h, int(n_ape), int(ckpt), ctypes.byref(lev), ctypes.byref(nb)))
@@ -497,6 +508,22 @@ class Batch:
         b = ctypes.c_int32()
         self._check(self.lib.su2g_batch_autotune(self.h, int(n_hb), int(n_or), ctypes.byref(b)))
         return b.value
+
+    MODES = {"graph": 0, "persistent": 1}
+
+    def configure(self, mode="graph", block=256):
+        """Run the sweeps as a replayed graph of per-pass launches or as one persistent launch."""
+        self._check(self.lib.su2g_batch_configure(self.h, self.MODES[mode], int(block)))
+
+    def selftest_grid_barrier(self, missing=1, wait_cycles=100_000_000):
+        """The persistent form's bounded barrier waiting for `missing` CTAs that do not exist; raises
+        Su2gError (SU2G_EDEVICE) when the wait runs out, as designed."""
+        self._check(self.lib.su2g_batch_selftest_grid_barrier(self.h, int(missing), int(wait_cycles)))
+
+    def config(self):
+        m, b = ctypes.c_int32(), ctypes.c_int32()
+        self._check(self.lib.su2g_batch_config(self.h, ctypes.byref(m), ctypes.byref(b)))
+        return {v: k for k, v in self.MODES.items()}[m.value], b.value
 
     def download(self, r):
         V = int(np.prod(self.replicas[r]["dims"]))

@@ -116,3 +116,58 @@ def test_fp32_adjoint_tracks_fp64_adjoint(thermalized_8):
     rel = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
     print("FP32 vs FP64 adjoint: relative L2 error", rel, "dQ", abs(q32 - q64))
     assert rel < 1e-4
+
+
+# ---- the adjoint configuration of the throughput runs: 24^4 and 48^4 hot starts thermalised by 500
+# sweeps (1 heatbath + 4 overrelaxation) at beta = 3.09, N = 30 APE_all steps at alpha = 0.5, then Q.
+# The perturbation exp(+-eps X) U runs on the device (su2g_tangent_step) after one upload of the base
+# field, so a central difference costs two uploads and two forwards.
+
+def _thermalised(L_, seed):
+    L = Lattice((L_,) * 4, precision="fp64", beta=3.09, seed=seed, start="haar")
+    L.sweep(500, 1, 4)
+    U = L.download()
+    L.close()
+    return U
+
+
+def _fd(L, U, X, n_ape, alpha):
+    qs = []
+    for sgn in (1.0, -1.0):
+        L.upload(U)
+        L.tangent_step(X, sgn * EPS)
+        L.ape(n_ape, alpha, "all")
+        qs.append(L.qtop())
+    return (qs[0] - qs[1]) / (2 * EPS)
+
+
+@pytest.mark.parametrize("L_,n_dirs", [(24, 16), (48, 4)])
+def test_vjp_matches_finite_differences_at_throughput_sizes(L_, n_dirs):
+    """FP64 VJP against FP64 central differences (eps = 1e-4) along N(0,1) su(2) directions, to 1e-6 of
+    max(|FD|, the size of the terms of sum g.x); the FP32 VJP (same field rounded to FP32) against the
+    same FP64 differences, to 2e-3 of that size (the FP32 VJP's error, ~1e-4 relative in L2, is the
+    FP32 rounding of 30 smearing levels propagated backwards)."""
+    n_ape, alpha = 30, 0.5
+    U = _thermalised(L_, 5000 + L_)
+    L64 = Lattice((L_,) * 4, precision="fp64")
+    L64.upload(U)
+    q64, g64 = L64.ape_qtop_vjp(n_ape, alpha)
+    L32 = Lattice((L_,) * 4, precision="fp32")
+    L32.upload(U)
+    q32, g32 = L32.ape_qtop_vjp(n_ape, alpha)
+    L32.close()
+    rng = np.random.default_rng(300 + L_)
+    worst64 = worst32 = 0.0
+    for d in range(n_dirs):
+        X = rng.standard_normal((U.shape[0], 4, 3))
+        fd = _fd(L64, U, X, n_ape, alpha)
+        ad64, ad32 = float(np.sum(g64 * X)), float(np.sum(g32 * X))
+        scale = max(abs(fd), float(np.sqrt(np.sum((g64 * X) ** 2))))
+        worst64 = max(worst64, abs(fd - ad64) / scale)
+        worst32 = max(worst32, abs(fd - ad32) / scale)
+        print(f"{L_}^4 direction {d}: FD {fd:+.10e}  VJP fp64 {ad64:+.10e}  fp32 {ad32:+.10e}  (scale {scale:.3e})")
+    print(f"{L_}^4 N={n_ape}: Q fp64 {q64:+.9f} fp32 {q32:+.9f}; worst |FD - VJP| / scale: fp64 {worst64:.2e}, "
+          f"fp32 {worst32:.2e}")
+    L64.close()
+    assert worst64 <= 1e-6
+    assert worst32 <= 2e-3

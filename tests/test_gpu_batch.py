@@ -18,9 +18,16 @@ REPS = [
 ]
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_batch_equals_single_lattices(precision):
+@pytest.mark.parametrize("precision,mode,block", [("fp64", "graph", 256), ("fp32", "graph", 256),
+                                                  ("fp64", "persistent", 128), ("fp32", "persistent", 256),
+                                                  ("fp32", "persistent", 128)])
+def test_batch_equals_single_lattices(precision, mode, block):
+    """Both forms (replayed graph of per-pass launches, one persistent cooperative launch) give the fields
+    of single handles bit for bit; the persistent form packs the 4^4 and 6x4x4x8 replicas (128 and 192
+    links a pass) into shared CTAs."""
     B = Batch(REPS, precision=precision)
+    B.configure(mode, block)
+    assert B.config() == (mode, block)
     trace, _ = B.run(3, n_hb=1, n_or=2, meas_every=1)
     assert trace.shape == (3, len(REPS))
     for i, r in enumerate(REPS):
@@ -46,6 +53,9 @@ def test_autotune_leaves_the_chains_untouched():
     before = [B.download(i) for i in range(len(REPS))]
     block = B.autotune(1, 4)
     assert block in (64, 128, 256)
+    mode, blk = B.config()
+    assert blk == block and mode in ("graph", "persistent")
+    print("autotuned:", mode, block)
     for i in range(len(REPS)):
         assert np.array_equal(B.download(i), before[i])
     t1, _ = B.run(1, 1, 1, 1)
@@ -90,3 +100,18 @@ def test_batched_beats_sequential_handles():
     print(f"64 x 12^4: batched {t_bat * 1e3:.3f} ms/sweep, sequential {t_seq * 1e3:.3f} ms/sweep, "
           f"speed-up {t_seq / t_bat:.1f}x")
     assert t_seq / t_bat > 2.0
+
+
+def test_persistent_barrier_wait_is_bounded():
+    """The grid-wide barrier of the persistent form, made to wait for a CTA that does not exist, gives up
+    after its limit and reports it (SU2G_EDEVICE) without a fault; the batch keeps working."""
+    from masterarbeit_b200.su2g import Su2gError
+    B = Batch(REPS[:2], precision="fp32")
+    B.selftest_grid_barrier(missing=0)
+    with pytest.raises(Su2gError) as e:
+        B.selftest_grid_barrier(missing=1, wait_cycles=50_000_000)
+    assert e.value.code == -4 and b"grid-wide barrier" in B.lib.su2g_batch_last_error(B.h)
+    B.configure("persistent", 128)
+    trace, _ = B.run(2, 1, 1, 1)
+    assert np.all(np.isfinite(trace))
+    B.close()
