@@ -1,12 +1,14 @@
 #!/usr/bin/env python3
 """Throughput of the SU(2) pure-gauge hot path on B200 -- one JSON line on rank 0.
 
-Workload (the headline metric's configuration): a 48^4 SU(2) lattice at beta = 3.09, Haar-random
-(hot) start from Philox, links in FP32.  One step = one sweep of 1 checkerboard heatbath + 4
-overrelaxation passes over all 4V links, followed by the plaquette (the reference's
-qcd.c:54-60 loop: gaugefieldUpdate then plaquette).  `value` is heatbath+overrelaxation link
-updates per second over all GPUs (5 * 4V updates per step per GPU).  The same run also reports
-APE_all / spatial-APE steps per second, the FP64 figures, W(R<=9,T<=9) sweeps and Q per second.
+Headline (the reference's own update, in its precision): a 48^4 SU(2) lattice at beta = 3.09,
+Haar-random (hot) start from Philox, FP64 links.  One step = one checkerboard heatbath sweep over
+all 4V links followed by the plaquette (the reference's qcd.c:54-60 loop: gaugefieldUpdate, then
+plaquette).  `value` is heatbath link updates per second over all GPUs (4V per step per GPU);
+`e2e` is the same step through the C ABI with the field uploaded from pinned host memory each step.
+`extras` holds the FP32 figures (1 heatbath + 4 overrelaxation sweeps, APE, W, Q), their ratio to
+FP64, the error of FP32 against FP64 on a thermalised field, the batched replicas, the graph loop,
+one configuration's measurement and the 96^4 lattice.
 
 Multi-GPU: independent replicas (one lattice per GPU, different seed), no data-path collective;
 the job aggregate is the sum of per-GPU work divided by the slowest rank's time.
@@ -271,36 +273,41 @@ def cpu_reference_rate(dims, reps, warm, sites, procs=None):
     }
 
 
-def cpu_reference_kernels(gpu, dims, ref_dims=(24, 24, 24, 24)):
-    """The reference's own APE_all / APE spatial steps, W(R<=9, T<=9) set and Q, one process each on
-    one core, at `ref_dims` (timed by the reference's getTime), scaled per site to `dims`, beside the
-    GPU figures of the same run.  The processes run concurrently (one core each)."""
-    exe = ref_harness(ref_dims)
-    if not exe:
+def cpu_reference_kernels(gpu, dims, small=(24, 24, 24, 24)):
+    """The reference's own APE_all and spatial APE steps and its Q, timed on the workload's lattice,
+    and its W(R<=9, T<=9) set timed at `small` and scaled by the site count (at 48^4 the set takes
+    ~160 s on one core); one process each on one core, run concurrently, timed by the reference's
+    getTime.  Beside them, the GPU figures of the same run."""
+    exe, exe_small = ref_harness(dims), ref_harness(small)
+    if not exe or not exe_small:
         return None
-    jobs = {"ape_all": ["bench_ape", "all", "0.5", "3"], "ape_spatial": ["bench_ape", "spatial", "0.5", "3"],
-            "wilson_R9T9": ["bench_wil", "9", "9", "1"], "qtop": ["bench_qtop", "1"]}
-    ps = {k: subprocess.Popen([exe] + a, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, cwd="/tmp")
-          for k, a in jobs.items()}
-    scale = math.prod(dims) / math.prod(ref_dims)
-    out = {"ref_dims": list(ref_dims), "note": "single-core reference time per unit at ref_dims, scaled by the "
-                                               "site count to the workload; GPU rates from this run"}
+    jobs = {"ape_all": (exe, ["bench_ape", "all", "0.5", "2"], dims),
+            "ape_spatial": (exe, ["bench_ape", "spatial", "0.5", "2"], dims),
+            "qtop": (exe, ["bench_qtop", "1"], dims),
+            "wilson_R9T9": (exe_small, ["bench_wil", "9", "9", "1"], small)}
+    # the harness writes the reference's log file into its working directory: a private temporary one
+    tmp = tempfile.TemporaryDirectory(prefix="su2ref_")
+    ps = {k: (subprocess.Popen([e] + a, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, cwd=tmp.name), d)
+          for k, (e, a, d) in jobs.items()}
+    out = {"dims": list(dims), "note": f"single-core reference time per unit; W timed at {'x'.join(map(str, small))} "
+                                       "and scaled by the site count, the others timed at dims; GPU rates from this run"}
     gpu_rate = {"ape_all": "ape_all_steps_per_s", "ape_spatial": "ape_spatial_steps_per_s",
                 "wilson_R9T9": "wilson_R9T9_sweeps_per_s", "qtop": "qtop_per_s"}
-    for k, p in ps.items():
+    for k, (p, d) in ps.items():
         txt, _ = p.communicate()
         ts = [float(line.split()[3]) for line in txt.splitlines() if line.startswith("RESULT") and line.split()[1]
               .endswith("_s")]
         if p.returncode != 0 or not ts:
             continue
-        t_ref = min(ts) * scale
-        e = {"cpu_ref_s_per_unit": t_ref}
+        t_ref = min(ts) * math.prod(dims) / math.prod(d)
+        e = {"cpu_ref_s_per_unit": t_ref, "timed_at": list(d)}
         for prec in ("fp64", "fp32"):
             r = gpu.get(f"{prec}_{gpu_rate[k]}")
             if r:
                 e[f"gpu_{prec}_s_per_unit"] = 1.0 / r
                 e[f"speedup_{prec}_vs_1_core"] = t_ref * r
         out[k] = e
+    tmp.cleanup()
     return out
 
 
@@ -413,6 +420,145 @@ def graph_figures(dist, sweeps=200):
     return out
 
 
+def kernel_rate(L, K, fn, cls, units, bytes_per_unit, peak):
+    """Plain-call rate of `fn` (K calls) and the CUDA-event duration of its `cls` launches (a second
+    pass with every launch bracketed by events): (units per second, GB/s, fraction of peak)."""
+    ms = time_steps(L, K, fn)
+    L.profile(True)
+    time_steps(L, K, fn)
+    n, tms = L.profile_read()[cls]
+    L.profile(False)
+    gbs = units * bytes_per_unit / (tms / n / 1e3) / 1e9
+    return K / (ms / 1e3), gbs, gbs / peak
+
+
+def precision_figures(L, prec, dims, K, W, peak, clk, extras):
+    """Throughput of every kernel of the path on lattice L of precision `prec`: the 1 HB + 4 OR step,
+    the heatbath-only sweep, APE all / spatial, W(R<=9, T<=9) and Q."""
+    vol = math.prod(dims)
+    lb = 16 if prec == "fp32" else 32
+    step = lambda: (L.sweep(1, 1, N_OR), L.plaquette())
+    for _ in range(W):
+        step()
+    ms = time_steps(L, K, step)
+    extras[f"{prec}_1hb{N_OR}or_link_updates_per_s"] = (1 + N_OR) * 4 * vol * K / (ms / 1e3)
+    L.profile(True)
+    time_steps(L, K, step)
+    prof = L.profile_read()
+    L.profile(False)
+    for cls, transfers in (("overrelax", 9), ("heatbath", 8)):
+        n, tms = prof[cls]
+        gbs = (vol // 2) * transfers * lb / (tms / n / 1e3) / 1e9
+        extras[f"{prec}_{cls}_pass_gbs"] = gbs
+        extras[f"{prec}_{cls}_pass_frac_of_peak"] = gbs / peak
+    hb = lambda: (L.sweep(1, 1, 0), L.plaquette())
+    ms = time_steps(L, K, hb)
+    extras[f"{prec}_heatbath_link_updates_per_s"] = 4 * vol * K / (ms / 1e3)
+    for mode, per_site in (("all", 8), ("spatial", 6)):
+        L.ape(1, 0.5, mode)
+        rate, gbs, frac = kernel_rate(L, K, lambda: L.ape(1, 0.5, mode), "ape", vol, per_site * lb, peak)
+        extras[f"{prec}_ape_{mode}_steps_per_s"] = rate
+        extras[f"{prec}_ape_{mode}_gbs"] = gbs
+        extras[f"{prec}_ape_{mode}_frac_of_peak"] = frac
+    R = [r for r in range(1, 10) for t in range(1, 10)]
+    T = [t for r in range(1, 10) for t in range(1, 10)]
+    # ALU-bound rows: algorithmic flops (line method: 765 quaternion products per site for R, T <= 9;
+    # clover charge: 576 products per site; 28 flop a product) against the nominal FP32 / FP64 rate of
+    # 148 SMs x 128 / 64 lanes x 2 flop at the SM clock sampled in the headline's timed region
+    f_mhz = (clk or {}).get("sm_mhz") or 1965.0
+    alu_peak = 148 * (128 if prec == "fp32" else 64) * 2 * f_mhz * 1e6
+    extras[f"{prec}_alu_peak_tflops_nominal"] = alu_peak / 1e12
+    L.wilson([1], [1])
+    ms_w = time_steps(L, 3, lambda: L.wilson(R, T)) / 3
+    extras[f"{prec}_wilson_R9T9_sweeps_per_s"] = 1e3 / ms_w
+    extras[f"{prec}_wilson_R9T9_frac_of_alu_peak"] = vol * 765 * 28 / (ms_w / 1e3) / alu_peak
+    L.qtop()
+    ms_q = time_steps(L, 3, L.qtop) / 3
+    extras[f"{prec}_qtop_per_s"] = 1e3 / ms_q
+    extras[f"{prec}_qtop_frac_of_alu_peak"] = vol * 576 * 28 / (ms_q / 1e3) / alu_peak
+
+
+def fp32_error_table(dims, device, seed):
+    """Error of the FP32 path against FP64 on one thermalised field (200 sweeps of 1 HB + 4 OR in FP64
+    from a Haar start, uploaded into both precisions): the plaquette, W(R <= 10, T <= 16) after 100 /
+    200 / 400 spatial APE steps and Q after 15 / 30 APE_all steps (alpha 0.5)."""
+    from masterarbeit_b200.su2g import Lattice
+    L64 = Lattice(dims, precision="fp64", beta=BETA, seed=seed, start="haar", device=device)
+    L64.sweep(200, 1, N_OR)
+    U = L64.download()
+    L32 = Lattice(dims, precision="fp32", beta=BETA, device=device)
+    L32.upload(U)
+    p32, p64 = L32.plaquette(), L64.plaquette()
+    out = {"field": f"{'x'.join(map(str, dims))} FP64 field after 200 sweeps of 1 HB + {N_OR} OR (Haar start), "
+                    "rounded to FP32 for the FP32 path", "plaquette_rel": abs(p32 - p64) / abs(p64)}
+    R = [r for r in range(1, 11) for t in range(1, 17)]
+    T = [t for r in range(1, 11) for t in range(1, 17)]
+    for n in (100, 200, 400):
+        w32 = L32.measure(R=R, T=T, ns_s=n, alpha_s=0.5)[1]
+        w64 = L64.measure(R=R, T=T, ns_s=n, alpha_s=0.5)[1]
+        d = abs(w32 - w64)
+        big = abs(w64) >= 1e-2
+        out[f"wilson_after_{n}_spatial_ape"] = {
+            "max_rel_where_W_ge_1e-2": float((d[big] / abs(w64[big])).max()), "loops_W_ge_1e-2": int(big.sum()),
+            "max_abs": float(d.max()), "max_rel_all": float((d / abs(w64)).max()),
+            "W10_16_fp64": float(w64[-1]), "W10_16_rel": float(d[-1] / abs(w64[-1]))}
+    q32 = L32.measure(q_ape=[15, 30], alpha_q=0.5)[0]
+    q64 = L64.measure(q_ape=[15, 30], alpha_q=0.5)[0]
+    for i, n in enumerate((15, 30)):
+        L64.upload(U)
+        L64.ape(n, 0.5, "all")
+        sabs = L64.qtop(with_abs=True)[1]
+        out[f"qtop_after_{n}_ape_all"] = {"q_fp64": float(q64[i]), "abs": float(abs(q32[i] - q64[i])),
+                                          "abs_over_sum_abs_q": float(abs(q32[i] - q64[i]) / sabs),
+                                          "rel": float(abs(q32[i] - q64[i]) / max(abs(q64[i]), 1e-300))}
+    out["meets_1e-6_relative"] = {
+        "plaquette": out["plaquette_rel"] <= 1e-6,
+        "wilson_W_ge_1e-2": all(out[f"wilson_after_{n}_spatial_ape"]["max_rel_where_W_ge_1e-2"] <= 1e-6
+                                for n in (100, 200, 400)),
+        "wilson_all": all(out[f"wilson_after_{n}_spatial_ape"]["max_rel_all"] <= 1e-6 for n in (100, 200, 400)),
+        "qtop": all(out[f"qtop_after_{n}_ape_all"]["rel"] <= 1e-6 for n in (15, 30))}
+    L32.close()
+    L64.close()
+    return out
+
+
+def big_lattice_figures(device, seed, K=3):
+    """96^4 (84.9 M sites): the sweeps and APE steps in both precisions, and one configuration of the
+    thesis' 96^4 measurement (400 spatial APE steps, then W(R <= 12, T <= 20)) in FP32, beside the
+    reference's logged time for it (measurements/96x96x96x96_SU2_b3.09_NAPE_400.meas)."""
+    from masterarbeit_b200.su2g import Lattice
+    dims = (96, 96, 96, 96)
+    vol = math.prod(dims)
+    out = {"dims": list(dims)}
+    for prec in ("fp32", "fp64"):
+        L = Lattice(dims, precision=prec, beta=BETA, seed=seed, start="haar", device=device)
+        L.sweep(1, 1, N_OR)
+        ms = time_steps(L, K, lambda: L.sweep(1, 1, 0))
+        out[f"{prec}_heatbath_link_updates_per_s"] = 4 * vol * K / (ms / 1e3)
+        ms = time_steps(L, K, lambda: L.sweep(1, 1, N_OR))
+        out[f"{prec}_1hb{N_OR}or_link_updates_per_s"] = (1 + N_OR) * 4 * vol * K / (ms / 1e3)
+        for mode in ("all", "spatial"):
+            L.ape(1, 0.5, mode)
+            ms = time_steps(L, K, lambda: L.ape(1, 0.5, mode))
+            out[f"{prec}_ape_{mode}_steps_per_s"] = K / (ms / 1e3)
+        if prec == "fp32":
+            R = [r for r in range(1, 13) for t in range(1, 21)]
+            T = [t for r in range(1, 13) for t in range(1, 21)]
+            spec = dict(R=R, T=T, ns_s=400, alpha_s=0.5)
+            L.measure(**spec)
+            L.synchronize()
+            t0 = time.perf_counter()
+            L.measure(**spec)
+            out["fp32_measurement_s_per_configuration"] = time.perf_counter() - t0
+            out["measurement_spec"] = "400 spatial APE steps (alpha 0.5), then W(R <= 12, T <= 20)"
+            out["reference_logged_s_per_configuration"] = 56715.0
+            out["reference_logged_source"] = ("measurements/96x96x96x96_SU2_b3.09_NAPE_400.meas (thesis cluster, one "
+                                              "core; 400 spatial APE + W(R <= 12, T <= 20) per configuration)")
+            L.measure_release()
+        L.close()
+    return out
+
+
 def run_ours(args, dist, dims):
     from masterarbeit_b200.su2g import Lattice, PinnedArray
 
@@ -420,10 +566,12 @@ def run_ours(args, dist, dims):
     vol = math.prod(dims)
     rank = dist.rank
     peak, peak_kind = measured_peak()
-    lat = Lattice(dims, precision="fp32", beta=BETA, seed=1000 + rank, start="haar", replica=rank, device=dist.local)
+    # the headline: the reference's own update in the reference's precision -- one FP64 checkerboard
+    # heatbath sweep of all 4V links, then the plaquette (qcd.c:54-60: gaugefieldUpdate, plaquette)
+    lat = Lattice(dims, precision="fp64", beta=BETA, seed=1000 + rank, start="haar", replica=rank, device=dist.local)
 
     def step():
-        lat.sweep(1, 1, N_OR)
+        lat.sweep(1, 1, 0)
         lat.plaquette()
 
     for _ in range(W):
@@ -442,35 +590,35 @@ def run_ours(args, dist, dims):
     lat.profile(False)
     dist.barrier()
     ms_max = dist.max(ms)
-    upd_per_step = (1 + N_OR) * 4 * vol
+    upd_per_step = 4 * vol
     value = upd_per_step * K * dist.world / (ms_max / 1e3)
     launches = sum(n for n, _ in prof.values())
-    link32 = 16
-    roof = {}
-    for name, cls, units, transfers in (("overrelax", "overrelax", vol // 2, 9), ("heatbath", "heatbath", vol // 2, 8)):
-        n, tms = prof[cls]
-        if n:
-            avg = tms / n
-            alg = units * transfers * link32
-            roof[name] = {"achieved_gbs": alg / (avg / 1e3) / 1e9, "avg_launch_ms": avg, "launches": n,
-                          "alg_bytes_per_launch": alg}
-    dom = roof.get("overrelax", {})
-    traffic = dram_traffic("overrelax_fp32_" + "x".join(map(str, dims)))
+    link64 = 32
+    n_hb, t_hb = prof["heatbath"]
+    avg = t_hb / n_hb
+    alg = (vol // 2) * 8 * link64
+    achieved = alg / (avg / 1e3) / 1e9
+    traffic = dram_traffic("heatbath_fp64_" + "x".join(map(str, dims)))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic: Philox Haar-random hot start (no checkpoints or datasets)",
-        "config": {"workload": f"{'x'.join(map(str, dims))} SU(2) beta={BETA} hot start; step = 1 heatbath + "
-                               f"{N_OR} overrelaxation checkerboard sweeps + plaquette",
-                   "dims": list(dims), "precision": "fp32 links, fp64 reductions",
-                   "l2": f"inputs larger than L2 (field {4 * vol * link32 / 1e6:.0f} MB > 126 MB)",
+        "dtype": "f64", "data": "synthetic: Philox Haar-random hot start (no checkpoints or datasets)",
+        "config": {"workload": f"{'x'.join(map(str, dims))} SU(2) beta={BETA} hot start; step = 1 checkerboard "
+                               "heatbath sweep (heatbath only, as the reference) + plaquette",
+                   "dims": list(dims), "precision": "fp64 links and arithmetic, as the reference",
+                   "l2": f"inputs larger than L2 (field {4 * vol * link64 / 1e6:.0f} MB > 126 MB)",
                    "parallelism": f"replicas x{dist.world}"},
-        "roofline": {"bound": "hbm", "kernel": "overrelaxation pass (32 of 40 passes per step)",
-                     "achieved": dom.get("achieved_gbs"), "peak": peak, "unit": "GB/s",
-                     "frac": (dom["achieved_gbs"] / peak) if dom else None, "traffic": traffic,
+        "roofline": {"bound": "hbm", "kernel": "FP64 heatbath pass k_update<double, mu, 0> (8 of the 8 update "
+                                              "launches of a step)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6650 GB/s",
-                     "alg_bytes_per_launch": dom.get("alg_bytes_per_launch"), "per_kernel": roof,
+                     "alg_bytes_per_launch": alg,
+                     "alg_bytes_note": "Vh = V/2 links updated; per update 8 links of 32 B move (the 6 staple "
+                                       "links of the three other directions, read, counted once per site over both "
+                                       "parity passes: 3V links; U_mu of the other parity: V/2; the update "
+                                       "written: V/2)",
+                     "avg_launch_ms": avg, "launches": n_hb,
                      "timing": "per-kernel CUDA-event durations from a second pass of the same K steps with "
                                "every launch bracketed by events; value and ms_per_step from the plain pass",
                      "ms_per_step_with_events": ms_instr / K},
@@ -480,82 +628,47 @@ def run_ours(args, dist, dims):
 
     extras = {}
     if not args.no_extras:
-        # APE steps/s (FP32) and the FP64 plain form of every figure
         for prec in ("fp32", "fp64"):
-            L = lat if prec == "fp32" else Lattice(dims, precision="fp64", beta=BETA, seed=1000 + rank,
+            L = lat if prec == "fp64" else Lattice(dims, precision="fp32", beta=BETA, seed=1000 + rank,
                                                     start="haar", replica=rank, device=dist.local)
-            lb = 16 if prec == "fp32" else 32
-            if prec == "fp64":
-                for _ in range(W):
-                    L.sweep(1, 1, N_OR)
-                k64 = max(3, K // 2)
-                step64 = lambda: (L.sweep(1, 1, N_OR), L.plaquette())
-                ms64 = time_steps(L, k64, step64)   # plain calls, like the FP32 headline
-                L.profile(True)
-                time_steps(L, k64, step64)          # event-bracketed: the per-kernel durations
-                p64 = L.profile_read()
-                L.profile(False)
-                extras["fp64_link_updates_per_s"] = upd_per_step * k64 / (ms64 / 1e3)
-                n, tms = p64["overrelax"]
-                extras["fp64_overrelax_gbs"] = (vol // 2) * 9 * lb / (tms / n / 1e3) / 1e9
-            for mode, per_site in (("all", 8), ("spatial", 6)):
-                L.ape(1, 0.5, mode)
-                ms_ape = time_steps(L, K, lambda: L.ape(1, 0.5, mode))   # plain calls
-                L.profile(True)
-                time_steps(L, K, lambda: L.ape(1, 0.5, mode))            # event-bracketed
-                pa = L.profile_read()
-                L.profile(False)
-                n, tms = pa["ape"]
-                extras[f"{prec}_ape_{mode}_steps_per_s"] = K / (ms_ape / 1e3)
-                extras[f"{prec}_ape_{mode}_gbs"] = vol * per_site * lb / (tms / n / 1e3) / 1e9
-                extras[f"{prec}_ape_{mode}_frac_of_peak"] = extras[f"{prec}_ape_{mode}_gbs"] / peak
-            R = [r for r in range(1, 10) for t in range(1, 10)]
-            T = [t for r in range(1, 10) for t in range(1, 10)]
-            # ALU-bound rows: algorithmic flops (line method: 765 quaternion products per site for
-            # R, T <= 9; clover charge: 576 products per site; 28 flop a product) against the nominal
-            # FP32 / FP64 rate of 148 SMs x 128 / 64 lanes x 2 flop at the SM clock sampled above
-            f_mhz = (clk or {}).get("sm_mhz") or 1965.0
-            alu_peak = 148 * (128 if prec == "fp32" else 64) * 2 * f_mhz * 1e6
-            extras[f"{prec}_alu_peak_tflops_nominal"] = alu_peak / 1e12
-            L.wilson([1], [1])
-            ms_w = time_steps(L, 1, lambda: L.wilson(R, T))
-            extras[f"{prec}_wilson_R9T9_sweeps_per_s"] = 1e3 / ms_w
-            extras[f"{prec}_wilson_R9T9_frac_of_alu_peak"] = vol * 765 * 28 / (ms_w / 1e3) / alu_peak
-            L.qtop()
-            ms_q = time_steps(L, 1, L.qtop)
-            extras[f"{prec}_qtop_per_s"] = 1e3 / ms_q
-            extras[f"{prec}_qtop_frac_of_alu_peak"] = vol * 576 * 28 / (ms_q / 1e3) / alu_peak
-            if prec == "fp64":
+            precision_figures(L, prec, dims, K, W, peak, clk, extras)
+            if prec == "fp32":
                 L.close()
-        extras["fp32_over_fp64_link_updates"] = value / dist.world / extras["fp64_link_updates_per_s"]
-        extras["fp32_over_fp64_ape_all"] = extras["fp32_ape_all_steps_per_s"] / extras["fp64_ape_all_steps_per_s"]
-    if not args.no_extras:
+        for k in ("1hb4or_link_updates_per_s", "heatbath_link_updates_per_s", "ape_all_steps_per_s",
+                  "ape_spatial_steps_per_s", "wilson_R9T9_sweeps_per_s", "qtop_per_s"):
+            extras[f"fp32_over_fp64_{k}"] = extras[f"fp32_{k}"] / extras[f"fp64_{k}"]
+        extras["fp32_error_vs_fp64"] = fp32_error_table(dims, dist.local, 3000 + rank)
         extras["batch"] = batch_figures(dist)
         extras["graph_loop"] = graph_figures(dist)
         # one configuration's measurement (the 48^4 flows of the thesis: 400 spatial APE steps then
         # W(R<=9, T<=9); Q after 30 APE_all steps), one CUDA graph per configuration
+        L = Lattice(dims, precision="fp32", beta=BETA, seed=1000 + rank, start="haar", replica=rank, device=dist.local)
+        L.sweep(2, 1, N_OR)
         R9 = [r for r in range(1, 10) for t in range(1, 10)]
         T9 = [t for r in range(1, 10) for t in range(1, 10)]
         spec = dict(q_ape=[30], alpha_q=0.5, R=R9, T=T9, ns_t=0, alpha_t=0.0, ns_s=400, alpha_s=0.5)
-        lat.measure(**spec)
+        L.measure(**spec)
         reps = 3
-        lat.synchronize()
+        L.synchronize()
         t0 = time.perf_counter()
         for _ in range(reps):
-            lat.measure(**spec)
+            L.measure(**spec)
         extras["measurement_fp32_ms_per_configuration"] = (time.perf_counter() - t0) * 1e3 / reps
         extras["measurement_spec"] = "Q after 30 APE_all (alpha 0.5); W(R<=9, T<=9) after 400 spatial APE (alpha 0.5)"
-        lat.measure_release()
+        L.measure_release()
+        L.close()
+        extras["lattice_96x96x96x96"] = big_lattice_figures(dist.local, 4000 + rank)
     line["extras"] = extras
 
     # end to end through the C ABI with host buffers: upload the configuration from pinned host
-    # memory (the reference's pu block, FP64 AoS), one step, read back the plaquette
+    # memory (the reference's pu block, FP64 AoS), one heatbath sweep with its acceptance, read back
+    # the plaquette
     host = PinnedArray((vol, 4, 4))
     lat.download(host.array)
 
     def e2e_step():
         lat.upload(host.array)
-        lat.sweep(1, 1, N_OR)
+        lat.sweep(1, 1, 0, acc=True)
         lat.plaquette()
 
     e2e_step()
@@ -565,9 +678,10 @@ def run_ours(args, dist, dims):
     wall_e2e = time.perf_counter() - t0
     ms_e2e = dist.max(ms_e2e)
     line["e2e"] = {"value": upd_per_step * K * dist.world / (ms_e2e / 1e3), "unit": UNIT,
-                   "h2d_bytes_per_step": vol * 16 * 8, "d2h_bytes_per_step": 8 + 4,
+                   "h2d_bytes_per_step": vol * 16 * 8, "d2h_bytes_per_step": 8 + 8,
                    "host_wall_s": wall_e2e,
-                   "what": "su2g_upload_aos_f64 (pinned host FP64 field) + su2g_sweep(1 HB + 4 OR) + su2g_plaquette"}
+                   "what": "su2g_upload_aos_f64 (pinned host FP64 field, the reference's pu block) + "
+                           "su2g_sweep(1 heatbath, acceptance read back) + su2g_plaquette (read back)"}
     host.free()
 
     if rank == 0 and dist.world == 1 and not args.no_cpu:
