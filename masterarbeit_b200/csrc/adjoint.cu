@@ -376,7 +376,7 @@ int vjp_t(su2g_lattice* h, int n_ape, double alpha, int c, double* q_out, double
         if ((rc = ape_step(h, cur, dst, SU2G_APE_ALL, alpha))) return rc;
         cur = dst;
     }
-    if ((rc = qtop_enqueue(h, cur, 0))) return rc;
+    if ((rc = ensure_lines(h)) || (rc = qtop_enqueue(h, cur, 0))) return rc;
     // G_N = dQ/dU_N
     const R scale = R(16.0 / (32.0 * kPi * kPi));
     Field<R> UN = make_field<R>(cur, g.Vh);

@@ -409,6 +409,7 @@ extern "C" int su2g_destroy(su2g_lattice* h)
     release_run_graph(h);
     release_meas_graph(h);
     if (h->pool) cudaMemPoolDestroy(h->pool);
+    cudaFree(h->lines);
     cudaFree(h->meas_work);
     cudaFree(h->meas_alt);
     cudaFree(h->d_run_ctr);

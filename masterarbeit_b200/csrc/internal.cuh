@@ -142,6 +142,7 @@ struct su2g_lattice {
     } run;
     cudaMemPool_t pool = nullptr;      // scratch of the adjoint; keeps its memory until destroy
     su2g_meas_graph* meas = nullptr;   // graph of one su2g_measure spec
+    void* lines = nullptr;             // 2- and 3-link line products of the field Q is measured on
     void* meas_work = nullptr;         // measurement copy of the field and its ping-pong partner
     void* meas_alt = nullptr;
     uint32_t* d_run_ctr = nullptr;   // [0] heatbath sweep index, [1] trace row (advanced by the graph)
@@ -195,7 +196,9 @@ int ape_step(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], i
 // TMA-tiled APE_all (FP32): rows per CTA if it applies to the geometry, else 0; and its launch.
 int ape_tma_rows(const Geom& g, int max_smem);
 int ape_tma_launch(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], double alpha, int yb);
-// Enqueue Q of the field at dirs; Q and sum|q| land in d_out[out_off], d_out[out_off + 1].
+// Scratch of the charge kernel (two fields of line products); allocate before any capture.
+int ensure_lines(su2g_lattice* h);
+// Enqueue Q of the field at dirs (ensure_lines first); Q and sum|q| land in d_out[out_off], d_out[out_off + 1].
 int qtop_enqueue(su2g_lattice* h, void* const dirs[4], int out_off);
 // FP64 AoS staging (the reference's pu layout) and the conversions of sites [n0, n0 + count)
 // between a device AoS buffer and the handle's field.

@@ -192,6 +192,7 @@ extern "C" int su2g_measure(su2g_lattice* h, const su2g_meas_spec* sp, double* q
         if ((rc = ensure_work(h))) return rc;
         if ((rc = ensure_partials(h, 8 * 32))) return rc;
         if ((rc = ensure_partial_entries(h, 2 * (size_t)((h->g.V + kBlock - 1) / kBlock)))) return rc;
+        if (sp->n_q > 0 && (rc = ensure_lines(h))) return rc;
         if ((rc = capture(h, sp))) return rc;
     }
     if ((rc = check_cuda(h, cudaGraphLaunch(h->meas->exec, h->stream), "replaying the measurement graph"))) return rc;

@@ -240,7 +240,8 @@ __device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g,
     const int n = t * g.S[0] + s;
     const Site st = site_lex(g, n, par);
     Q<R>* own = line + (size_t)threadIdx.x * RC;
-    int xr[RC];   // lexicographic index of x + (r0 + r) k
+    int xr[RC];    // lexicographic index of x + (r0 + r) k
+    Q<R> SX[RC];   // the thread's own spatial lines, kept in registers across the T loop
     Q<R> S = q_one<R>();
     for (int jj = 0; jj < r0 - 1; ++jj) S = q_mul(S, U.ld(K, par ^ (jj & 1), n + shift_k<K>(g, st.c[K], jj)));
 #pragma unroll
@@ -248,6 +249,7 @@ __device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g,
         const int jj = r0 - 1 + r;
         S = q_mul(S, U.ld(K, par ^ (jj & 1), n + shift_k<K>(g, st.c[K], jj)));
         own[r] = S;
+        SX[r] = S;
         xr[r] = n + shift_k<K>(g, st.c[K], jj + 1);
     }
     __syncthreads();
@@ -266,7 +268,7 @@ __device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g,
         const Q<R>* other = line + (size_t)(tt * sw + j) * RC;   // S_{r0+r}(x + T t)
 #pragma unroll
         for (int r = 0; r < RC; ++r) {
-            const R w = valid ? q_dot(q_mul(TX, other[r]), q_mul(own[r], TR[r])) : R(0);
+            const R w = valid ? q_dot(q_mul(TX, other[r]), q_mul(SX[r], TR[r])) : R(0);
             wilson_acc<R>(wacc, w, wilson_slot<R>(r, T - tlo, nT, warp), lane);
         }
     }
@@ -333,28 +335,105 @@ size_t wilson_col_smem(int threads, int nT)
 
 // --------------------------------------------------- topological charge ---
 
+// Line products for the charge: L^e_D(x) = U_D(x) U_D(x+D) ... U_D(x+(e-1)D) for e = 2, 3 and every
+// direction D, stored in the field's layout (L2 and L3 are two four-direction fields).  The clover
+// leaves of size e are then products of four e-link segments, each one line (computeLine,
+// topologicalcharge.c:18-44, evaluated once per segment and site instead of once per leaf).
+template <typename R>
+__global__ void __launch_bounds__(kBlock) k_lines(Field<R> U, Field<R> L2, Field<R> L3, Geom g)
+{
+    Site s;
+    int par, h;
+    if (!site_cta_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) return;
+#pragma unroll
+    for (int D = 0; D < 4; ++D) {
+        int c = s.c[D] + 1;
+        c -= c >= g.L[D] ? g.L[D] : 0;
+        const int n1 = s.n + (c - s.c[D]) * g.S[D];
+        int c2 = c + 1;
+        c2 -= c2 >= g.L[D] ? g.L[D] : 0;
+        const int n2 = s.n + (c2 - s.c[D]) * g.S[D];
+        const Q<R> l2 = q_mul(U.ldh(D, par, h), U.ld(D, par ^ 1, n1));
+        L2.sth(D, par, h, l2);
+        L3.sth(D, par, h, q_mul(l2, U.ld(D, par, n2)));
+    }
+}
+
+// Offset of the lexicographic index for k steps (|k| <= 3) along direction d from coordinate c.
+__device__ __forceinline__ int shift_by(const Geom& g, int d, int c, int k)
+{
+    int cc = c + k;
+    while (cc < 0) cc += g.L[d];
+    while (cc >= g.L[d]) cc -= g.L[d];
+    return (cc - c) * g.S[d];
+}
+
+// Improved clover field strength in plane (A, B) at site s from line products (the same
+// F = [(k1 C1 + k2 C2 + k3 C3) - h.c.]/2, C_e = (1/4) sum of the four e x e leaves, (k1, k2, k3) =
+// (1.5, -0.15, 1/90), as clover_F in clover.cuh; topologicalcharge.c:46-162).  With a = eA, b = eB
+// and L the e-link lines of the two directions, the leaves starting and ending at x are
+//   +A +B -A -B:  LA(x) LB(x+a) LA(x+b)^dag LB(x)^dag
+//   -B +A +B -A:  LB(x-b)^dag LA(x-b) LB(x+a-b) LA(x)^dag
+//   +B -A -B +A:  LB(x) LA(x-a+b)^dag LB(x-a)^dag LA(x-a)
+//   -A -B +A +B:  LA(x-a)^dag LB(x-a-b)^dag LA(x-a-b) LB(x-b)
+// : twelve loads and twelve products per size.
+template <typename R, int A, int B>
+__device__ __forceinline__ Q<R> clover_F_lines(const Field<R>& U, const Field<R>& L2, const Field<R>& L3,
+                                               const Geom& g, const Site& s, int par)
+{
+    Q<R> F = q_zero<R>();
+#pragma unroll 1
+    for (int e = 1; e <= 3; ++e) {
+        // the two directions' e-link lines (pointers selected in registers, not a field by reference)
+        Field<R> L;
+        L.Vh = U.Vh;
+        L.p[A] = e == 1 ? U.p[A] : (e == 2 ? L2.p[A] : L3.p[A]);
+        L.p[B] = e == 1 ? U.p[B] : (e == 2 ? L2.p[B] : L3.p[B]);
+        const R kcoef = e == 1 ? R(1.5) : (e == 2 ? R(-0.15) : R(1.0 / 90.0));
+        const int pa = A, pb = B;
+        const int oa = shift_by(g, pa, s.c[pa], e), ma = shift_by(g, pa, s.c[pa], -e);
+        const int ob = shift_by(g, pb, s.c[pb], e), mb = shift_by(g, pb, s.c[pb], -e);
+        const int q1 = par ^ (e & 1);   // parity one segment away
+        const int n = s.n;
+        const Q<R> LAx = L.ld(A, par, n), LBx = L.ld(B, par, n);
+        const Q<R> LBxa = L.ld(B, q1, n + oa), LAxb = L.ld(A, q1, n + ob);
+        const Q<R> LBxmb = L.ld(B, q1, n + mb), LAxmb = L.ld(A, q1, n + mb);
+        const Q<R> LBxamb = L.ld(B, par, n + oa + mb), LAxmab = L.ld(A, par, n + ma + ob);
+        const Q<R> LBxma = L.ld(B, q1, n + ma), LAxma = L.ld(A, q1, n + ma);
+        const Q<R> LBxmamb = L.ld(B, par, n + ma + mb), LAxmamb = L.ld(A, par, n + ma + mb);
+        const Q<R> l0 = q_mul_nd(q_mul_nd(q_mul(LAx, LBxa), LAxb), LBx);
+        const Q<R> l1 = q_mul_nd(q_mul(q_mul_dn(LBxmb, LAxmb), LBxamb), LAx);
+        const Q<R> l2 = q_mul(q_mul_nd(q_mul_nd(LBx, LAxmab), LBxma), LAxma);
+        const Q<R> l3 = q_mul(q_mul(q_dag(q_mul(LBxmamb, LAxma)), LAxmamb), LBxmb);
+        F = q_axpy(kcoef * R(0.25), q_add(q_add(l0, l1), q_add(l2, l3)), F);
+    }
+    F.c0 = R(0);   // (F - F^dag)/2 keeps the su(2) part
+    return F;
+}
+
 // q(x) = 8 [tr F01 F23 + tr F02 F31 + tr F03 F12], tr = 2 c0 (topologicalcharge.c:175-178)
 template <typename R>
-__device__ __forceinline__ double qtop_density(const Field<R>& U, const Geom& g, const Site& s, int par)
+__device__ __forceinline__ double qtop_density(const Field<R>& U, const Field<R>& L2, const Field<R>& L3,
+                                               const Geom& g, const Site& s, int par)
 {
     double d = 0.0;
-    d += 16.0 * (double)q_mul(clover_F<R, 0, 1>(U, g, s, par), clover_F<R, 2, 3>(U, g, s, par)).c0;
-    d += 16.0 * (double)q_mul(clover_F<R, 0, 2>(U, g, s, par), clover_F<R, 3, 1>(U, g, s, par)).c0;
-    d += 16.0 * (double)q_mul(clover_F<R, 0, 3>(U, g, s, par), clover_F<R, 1, 2>(U, g, s, par)).c0;
+    d += 16.0 * (double)q_mul(clover_F_lines<R, 0, 1>(U, L2, L3, g, s, par), clover_F_lines<R, 2, 3>(U, L2, L3, g, s, par)).c0;
+    d += 16.0 * (double)q_mul(clover_F_lines<R, 0, 2>(U, L2, L3, g, s, par), clover_F_lines<R, 3, 1>(U, L2, L3, g, s, par)).c0;
+    d += 16.0 * (double)q_mul(clover_F_lines<R, 0, 3>(U, L2, L3, g, s, par), clover_F_lines<R, 1, 2>(U, L2, L3, g, s, par)).c0;
     return d;
 }
 
 // One site per thread; CTA partials of q and |q| at partials[b] and partials[gridDim.x + b].
-// Resident CTAs per SM: three in FP32 (80 registers, no spill) and two in FP64 (126), measured at 48^4
-// on B200 against two and one: 282.9 against 267.6 Q/s in FP32, ~166 against ~157 in FP64.
+// Resident CTAs per SM: three in FP32 and two in FP64.
 template <typename R>
-__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 3 : 2) k_qtop(Field<R> U, Geom g, DD* __restrict__ partials)
+__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 3 : 2) k_qtop(Field<R> U, Field<R> L2, Field<R> L3, Geom g,
+                                                                        DD* __restrict__ partials)
 {
     // parities paired per warp (site_warp_pair); grid ceil(V / kBlock)
     Site s;
     int par, h;
     double d = 0.0;
-    if (site_warp_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) d = qtop_density<R>(U, g, s, par);
+    if (site_warp_pair(g, blockIdx.x, threadIdx.x, blockDim.x, s, par, h)) d = qtop_density<R>(U, L2, L3, g, s, par);
     DD acc = dd_block_sum_d<kBlock>(d);
     DD aabs = dd_block_sum_d<kBlock>(fabs(d));
     if (threadIdx.x == 0) {
@@ -494,16 +573,39 @@ int su2g::ape_enqueue(su2g_lattice* h, int ns, double alpha, int mode)
     return SU2G_OK;
 }
 
+int su2g::ensure_lines(su2g_lattice* h)
+{
+    if (h->lines) return SU2G_OK;
+    const cudaError_t e = cudaMalloc(&h->lines, 8ull * h->g.V * h->link_bytes);
+    if (e != cudaSuccess) return check_cuda(h, e, "allocating the charge's line products");
+    return SU2G_OK;
+}
+
 int su2g::qtop_enqueue(su2g_lattice* h, void* const dirs[4], int out_off)
 {
+    if (!h->lines) return set_error(h, SU2G_EINVAL, "topological charge: line scratch not allocated");
     const int grid = (int)((h->g.V + kBlock - 1) / kBlock);
     int rc0 = ensure_partial_entries(h, 2ull * grid);
     if (rc0) return rc0;
+    void* l2[4];
+    void* l3[4];
+    for (int mu = 0; mu < 4; ++mu) {
+        l2[mu] = (char*)h->lines + (size_t)mu * h->g.V * h->link_bytes;
+        l3[mu] = (char*)h->lines + (size_t)(4 + mu) * h->g.V * h->link_bytes;
+    }
+    const int lgrid = 2 * (int)((h->g.Vh + kBlock - 1) / kBlock);
     launch_begin(h, SU2G_K_QTOP);
-    if (h->prec == SU2G_FP32)
-        k_qtop<float><<<grid, kBlock, 0, h->stream>>>(make_field<float>(dirs, h->g.Vh), h->g, h->partials);
-    else
-        k_qtop<double><<<grid, kBlock, 0, h->stream>>>(make_field<double>(dirs, h->g.Vh), h->g, h->partials);
+    if (h->prec == SU2G_FP32) {
+        const Field<float> U = make_field<float>(dirs, h->g.Vh), L2 = make_field<float>(l2, h->g.Vh),
+                           L3 = make_field<float>(l3, h->g.Vh);
+        k_lines<float><<<lgrid, kBlock, 0, h->stream>>>(U, L2, L3, h->g);
+        k_qtop<float><<<grid, kBlock, 0, h->stream>>>(U, L2, L3, h->g, h->partials);
+    } else {
+        const Field<double> U = make_field<double>(dirs, h->g.Vh), L2 = make_field<double>(l2, h->g.Vh),
+                            L3 = make_field<double>(l3, h->g.Vh);
+        k_lines<double><<<lgrid, kBlock, 0, h->stream>>>(U, L2, L3, h->g);
+        k_qtop<double><<<grid, kBlock, 0, h->stream>>>(U, L2, L3, h->g, h->partials);
+    }
     int rc = launch_end(h, SU2G_K_QTOP, "topological charge kernel");
     // Q = sum_x q(x) / (32 pi^2)  (topologicalcharge.c:194)
     if (!rc) rc = finalize(h, grid, 2, 1.0 / (32.0 * kPi * kPi), out_off, grid);
@@ -629,7 +731,8 @@ extern "C" int su2g_qtop(su2g_lattice* h, double* q, double* sum_abs)
     if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_qtop: null handle");
     if (!q) return set_error(h, SU2G_EINVAL, "su2g_qtop: null output");
     cudaSetDevice(h->device);
-    int rc = qtop_enqueue(h, h->dirp, 0);
+    int rc = ensure_lines(h);
+    if (!rc) rc = qtop_enqueue(h, h->dirp, 0);
     if (!rc) rc = fetch_results(h, 0, 2);
     if (!rc) {
         *q = h->h_out[0];
