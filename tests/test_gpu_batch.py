@@ -23,7 +23,7 @@ REPS = [
                                                   ("fp32", "persistent", 128)])
 def test_batch_equals_single_lattices(precision, mode, block):
     """Both forms (replayed graph of per-pass launches, one persistent cooperative launch) give the fields
-    of single handles bit for bit; the persistent form packs the 4^4 and 6x4x4x8 replicas (128 and 192
+    of single handles bit for bit; the persistent form packs the 4^4 and 6x4x4x8 replicas (128 and 384
     links a pass) into shared CTAs."""
     B = Batch(REPS, precision=precision)
     B.configure(mode, block)
