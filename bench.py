@@ -366,8 +366,16 @@ def batch_figures(dist, sweeps=1000, seq_sweeps=20):
         upd = (1 + N_OR) * 4 * sum(L ** 4 for L in sizes)
         B = Batch(reps, precision="fp32", device=dist.local)
         block = B.autotune(1, N_OR)
+        mode, _ = B.config()
         B.run(10, 1, N_OR, 1)
         trace, ms = B.run(sweeps, 1, N_OR, 1)
+        # each form at each of its CTA widths, 200 sweeps (the autotuner's choice is the timed run above)
+        forms = {}
+        for fm, fb in (("graph", 64), ("graph", 128), ("graph", 256), ("persistent", 128), ("persistent", 256)):
+            B.configure(fm, fb)
+            B.run(5, 1, N_OR, 1)
+            _, fms = B.run(200, 1, N_OR, 1)
+            forms[f"{fm}_{fb}"] = upd / (fms / 200 / 1e3)
         B.close()
         ms_sweep_batch = ms / sweeps
         Ls = [Lattice(r["dims"], precision="fp32", beta=r["beta"], seed=r["seed"], start=r["start"],
@@ -384,6 +392,7 @@ def batch_figures(dist, sweeps=1000, seq_sweeps=20):
         for L in Ls:
             L.close()
         out[name] = {"replicas": len(sizes), "sites": sum(L ** 4 for L in sizes), "autotuned_block": block,
+                     "autotuned_form": mode, "link_updates_per_s_by_form": forms,
                      "sweeps": sweeps, "batched_ms_per_sweep": ms_sweep_batch,
                      "batched_link_updates_per_s": upd / (ms_sweep_batch / 1e3),
                      "sequential_ms_per_sweep": ms_sweep_seq, "speedup_vs_sequential": ms_sweep_seq / ms_sweep_batch,

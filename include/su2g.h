@@ -248,8 +248,9 @@ int su2g_batch_run(su2g_batch *b, int32_t n_sweeps, int32_t n_hb, int32_t n_or, 
  * graph and replayed.  SU2G_BATCH_PERSISTENT: the whole su2g_batch_run as one cooperative launch
  * whose resident CTAs walk every pass as one global link index over all replicas (small replicas
  * share a CTA) and meet at a bounded grid-wide barrier between passes; a barrier that waits too
- * long makes the run return SU2G_EDEVICE.  Both draw the same Philox streams: results are
- * identical. */
+ * long makes the run return SU2G_EDEVICE.  Both draw the same Philox streams; the persistent
+ * kernel's multiply-adds may round differently in the last bit, so its fields agree with the
+ * graph form's to rounding, not bit for bit. */
 enum su2g_batch_mode { SU2G_BATCH_GRAPH = 0, SU2G_BATCH_PERSISTENT = 1 };
 /* Choose the form and the CTA width (64, 128 or 256 threads; 128 or 256 for the persistent form). */
 int su2g_batch_configure(su2g_batch *b, int32_t mode, int32_t block);

@@ -17,8 +17,8 @@ observables of the thesis' measurement programs are computed in both: the plaque
 T <= 16) after 100, 200 and 400 spatial APE steps (alpha 0.5); Q after 15 and 30 APE_all steps
 (alpha 0.5).  Bounds, asserted:
   - plaquette: 1e-6 relative (well conditioned: a mean of 6V terms of one sign);
-  - W(R, T): |dW| <= 1e-6 relative where W >= 1e-2; for the small loops, whose mean is a sum of
-    site terms of both signs, |dW| <= 2e-8, i.e. 2e-8 of mean_x |w_x| <= 1;
+  - W(R, T): |dW| <= 1e-6 relative, or 1e-9 absolute for a loop whose mean falls below 1e-3 (a sum
+    of site terms of both signs, each |w_x| <= 1);
   - Q: |dQ| <= 1e-6 * sum_x |q_x| / (32 pi^2) (Q sums site densities of both signs).
 """
 import math
@@ -109,12 +109,13 @@ def test_fp32_error_against_fp64_on_thermalised_field():
     for n in (100, 200, 400):
         w = {p: L.measure(R=R, T=T, ns_s=n, alpha_s=0.5)[1] for p, L in h.items()}
         d = np.abs(w["fp32"] - w["fp64"])
-        big = np.abs(w["fp64"]) >= 1e-2
-        relw = d[big] / np.abs(w["fp64"][big])
-        print(f"W after {n} spatial APE: max relative error {relw.max():.2e} over {big.sum()} loops with W >= 1e-2; "
-              f"max |dW| {d.max():.2e} over all {len(d)} (smallest |W| {np.abs(w['fp64']).min():.1e})")
-        assert relw.max() <= 1e-6
-        assert d.max() <= 2e-8
+        rel = d / np.abs(w["fp64"])
+        print(f"W after {n} spatial APE: max relative error {rel.max():.2e} over all {len(d)} loops "
+              f"(smallest |W| {np.abs(w['fp64']).min():.1e}, W(10,16) {w['fp64'][-1]:.4e} to {rel[-1]:.1e}); "
+              f"max |dW| {d.max():.2e}")
+        # 1e-6 relative; for a loop whose mean falls below 1e-3 (a sum of site terms of both signs,
+        # each |w_x| <= 1) the bound becomes 1e-9 absolute
+        assert np.all(d <= 1e-6 * np.maximum(np.abs(w["fp64"]), 1e-3)), rel.max()
     q = {p: L.measure(q_ape=[15, 30], alpha_q=0.5)[0] for p, L in h.items()}
     # condition number of Q: sum_x |q_x| / (32 pi^2) on the FP64 field after the same smearing
     L64 = h["fp64"]
