@@ -38,6 +38,19 @@ FALLBACK_HBM_GBS = 6650.0
 
 # ------------------------------------------------------------------ helpers ---
 
+R9 = [r for r in range(1, 10) for t in range(1, 10)]
+T9 = [t for r in range(1, 10) for t in range(1, 10)]
+# one call of each kernel family on a lattice L (the --kernel mode)
+KERNELS = {
+    "heatbath": lambda L: L.sweep(1, 1, 0),
+    "overrelax": lambda L: L.sweep(1, 0, 1),
+    "plaquette": lambda L: L.plaquette(),
+    "ape_all": lambda L: L.ape(1, 0.5, "all"),
+    "ape_spatial": lambda L: L.ape(1, 0.5, "spatial"),
+    "wilson": lambda L: L.wilson(R9, T9),
+    "qtop": lambda L: L.qtop(),
+}
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -47,6 +60,10 @@ def parse():
     ap.add_argument("--dims", default="48,48,48,48")
     ap.add_argument("--no-extras", action="store_true", help="headline only")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--kernel", choices=sorted(KERNELS), default=None,
+                    help="time one kernel family alone on the workload lattice (for profiling): "
+                         "--steps calls after --warmup calls, one JSON line")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="precision for --kernel")
     return ap.parse_args()
 
 
@@ -707,9 +724,27 @@ def run_ours(args, dist, dims):
         print(json.dumps(line), flush=True)
 
 
+def run_kernel(args, dims):
+    """One kernel family alone: a Haar-start lattice after 2 sweeps of 1 HB + 4 OR, --warmup calls,
+    then --steps calls timed with CUDA events on the lattice's stream (a profiling target)."""
+    from masterarbeit_b200.su2g import Lattice
+    L = Lattice(dims, precision=args.precision, beta=BETA, seed=1000, start="haar")
+    L.sweep(2, 1, N_OR)
+    fn = KERNELS[args.kernel]
+    for _ in range(args.warmup):
+        fn(L)
+    ms = time_steps(L, max(1, args.steps), lambda: fn(L))
+    L.close()
+    print(json.dumps({"kernel": args.kernel, "precision": args.precision, "dims": dims, "calls": args.steps,
+                      "ms_per_call": ms / max(1, args.steps)}), flush=True)
+
+
 def main():
     args = parse()
     dims = [int(x) for x in args.dims.split(",")]
+    if args.kernel:
+        run_kernel(args, dims)
+        return
     dist = Dist()
     try:
         if args.impl == "reference":

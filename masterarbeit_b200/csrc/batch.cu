@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(256, 4) k_batch_update(const Replica* __restri
         uint32_t trials = 0;
         if (heatbath_link<R>(A, (R)rp.beta, rp.seed, (uint32_t)s.n, ctr[kCtrSweep] + sub, (uint32_t)MU, rp.id, trials,
                              out, status))
-            U.sth(MU, par, h, q_project(out));
+            U.sth(MU, par, h, hb_store(out));
     } else {
         U.sth(MU, par, h, q_project(overrelax_link<R>(A, U.ldh(MU, par, h))));
     }
@@ -331,7 +331,7 @@ __device__ __forceinline__ void persist_pass(const PersistArgs& a, const int* __
             uint32_t trials = 0;
             if (heatbath_link<R>(A, (R)rp.beta, rp.seed, (uint32_t)s.n, sweep, (uint32_t)MU, rp.id, trials, out,
                                  a.status))
-                U.sth(MU, par, h, q_project(out));
+                U.sth(MU, par, h, hb_store(out));
         } else {
             U.sth(MU, par, h, q_project(overrelax_link<R>(A, U.ldh(MU, par, h))));
         }

@@ -211,6 +211,11 @@ constexpr int kWilsonColMaxThreads = 512;
 template <typename R>
 __host__ __device__ constexpr bool wilson_thread_slots() { return sizeof(R) == 8; }
 
+// Quaternions of shared memory per thread and R in the column kernel: FP32 transports the loops
+// through two buffers, FP64 keeps one array of spatial lines.
+template <typename R>
+__host__ __device__ constexpr int wilson_col_bufs() { return sizeof(R) == 4 ? 2 : 1; }
+
 template <typename R>
 __device__ __forceinline__ size_t wilson_slot(int r, int ti, int nT, int warp)
 {
@@ -230,8 +235,58 @@ __device__ __forceinline__ void wilson_acc(double* __restrict__ wacc, R w, size_
     }
 }
 
+// The loops of one spatial direction K for a CTA's column, transported up in time:
+//   Y_R^T(x) = T_T(x) S_R(x + T t) T_T(x + R k)^dag = U_t(x) Y_R^{T-1}(x + t) U_t(x + R k)^dag,
+//   Y_R^0 = S_R,   W(R, T) at x = <Y_R^T(x), S_R(x)>  (compute_wloop, wilson.c:21-56, factored).
+// U_t(x + R k) does not depend on T, so the T loop loads nothing from global memory: Y^{T-1}(x + t)
+// is the value the thread one time slice up (thread (t+1) sw + j, periodic) wrote into a
+// double-buffered shared array, one barrier per T; two products per (R, T) and site.
 template <typename R, int K, int RC>
-__device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g, Q<R>* __restrict__ line,
+__device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g, Q<R>* __restrict__ ybuf,
+                                               double* __restrict__ wacc, int sw, int t, int j, int s, bool valid,
+                                               int r0, int tlo, int thi)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nT = thi - tlo + 1;
+    int par;
+    const int n = t * g.S[0] + s;
+    const Site st = site_lex(g, n, par);
+    Q<R> SX[RC], UR[RC], Y[RC];   // S_{r0+r}(x); U_t(x + (r0+r) k); the transported loop
+    Q<R> S = q_one<R>();
+    for (int jj = 0; jj < r0 - 1; ++jj) S = q_mul(S, U.ld(K, par ^ (jj & 1), n + shift_k<K>(g, st.c[K], jj)));
+#pragma unroll
+    for (int r = 0; r < RC; ++r) {
+        const int jj = r0 - 1 + r;
+        S = q_mul(S, U.ld(K, par ^ (jj & 1), n + shift_k<K>(g, st.c[K], jj)));
+        SX[r] = S;
+        Y[r] = S;
+        UR[r] = U.ld(0, par ^ ((jj + 1) & 1), n + shift_k<K>(g, st.c[K], jj + 1));
+    }
+    const Q<R> UT = U.ld(0, par, n);
+    int tn = t + 1;
+    tn -= tn >= g.L[0] ? g.L[0] : 0;
+    const size_t up = (size_t)(tn * sw + j) * RC, own = (size_t)threadIdx.x * RC;
+    for (int T = 1; T <= thi; ++T) {
+        Q<R>* buf = ybuf + (size_t)(T & 1) * blockDim.x * RC;
+#pragma unroll
+        for (int r = 0; r < RC; ++r) buf[own + r] = Y[r];
+        __syncthreads();   // the other buffer was last read before the previous barrier
+#pragma unroll
+        for (int r = 0; r < RC; ++r) Y[r] = q_mul_nd(q_mul(UT, buf[up + r]), UR[r]);
+        if (T < tlo) continue;
+#pragma unroll
+        for (int r = 0; r < RC; ++r) {
+            const R w = valid ? q_dot(Y[r], SX[r]) : R(0);
+            wilson_acc<R>(wacc, w, wilson_slot<R>(r, T - tlo, nT, warp), lane);
+        }
+    }
+    __syncthreads();   // the buffers are written again by the next direction
+}
+
+// FP64 form of the column sums: the temporal lines T_T(x) and T_T(x + R k) are built up per T and
+// the spatial line S_R(x + T t) is read from the shared-memory line array of the thread one T up
+// (the transported form above needs three RC-loop registers more, which spill in FP64).
+template <typename R, int K, int RC>
+__device__ __forceinline__ void wilson_col_dir_lines(const Field<R>& U, const Geom& g, Q<R>* __restrict__ line,
                                                double* __restrict__ wacc, int sw, int t, int j, int s, bool valid,
                                                int r0, int tlo, int thi)
 {
@@ -280,9 +335,9 @@ __global__ void __launch_bounds__(kWilsonColMaxThreads, 1) k_wilson_col(Field<R>
                                                                         int thi, DD* __restrict__ partials)
 {
     extern __shared__ __align__(16) unsigned char wsm[];
-    Q<R>* line = (Q<R>*)wsm;
+    Q<R>* ybuf = (Q<R>*)wsm;   // FP32: two buffers of RC loops per thread; FP64: RC spatial lines
     const int nwarps = blockDim.x >> 5, nT = thi - tlo + 1;
-    double* wacc = (double*)(wsm + (size_t)blockDim.x * RC * sizeof(Q<R>));
+    double* wacc = (double*)(wsm + (size_t)wilson_col_bufs<R>() * blockDim.x * RC * sizeof(Q<R>));
     const int owners = wilson_thread_slots<R>() ? (int)blockDim.x : nwarps;
     for (int i = threadIdx.x; i < owners * RC * nT; i += blockDim.x) wacc[i] = 0.0;
     __syncthreads();
@@ -292,9 +347,12 @@ __global__ void __launch_bounds__(kWilsonColMaxThreads, 1) k_wilson_col(Field<R>
         const int s_req = tile * sw + j;
         const bool valid = s_req < stot;
         const int s = valid ? s_req : stot - 1;   // threads past the end read a valid site and add 0
-        wilson_col_dir<R, 1, RC>(U, g, line, wacc, sw, t, j, s, valid, r0, tlo, thi);
-        wilson_col_dir<R, 2, RC>(U, g, line, wacc, sw, t, j, s, valid, r0, tlo, thi);
-        wilson_col_dir<R, 3, RC>(U, g, line, wacc, sw, t, j, s, valid, r0, tlo, thi);
+        if (sizeof(R) == 4) wilson_col_dir<R, 1, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
+        else wilson_col_dir_lines<R, 1, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
+        if (sizeof(R) == 4) wilson_col_dir<R, 2, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
+        else wilson_col_dir_lines<R, 2, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
+        if (sizeof(R) == 4) wilson_col_dir<R, 3, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
+        else wilson_col_dir_lines<R, 3, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
     }
     // fixed-order sum over warps; slot r * kWilsonTChunk + (T - tlo) as in k_wilson
     for (int i = threadIdx.x; i < RC * nT; i += blockDim.x) {
@@ -330,7 +388,7 @@ template <typename R, int RC>
 size_t wilson_col_smem(int threads, int nT)
 {
     const int owners = wilson_thread_slots<R>() ? threads : threads / 32;
-    return (size_t)threads * RC * sizeof(Q<R>) + (size_t)owners * RC * nT * sizeof(double);
+    return (size_t)wilson_col_bufs<R>() * threads * RC * sizeof(Q<R>) + (size_t)owners * RC * nT * sizeof(double);
 }
 
 // --------------------------------------------------- topological charge ---

@@ -94,6 +94,17 @@ __host__ __device__ __forceinline__ Q<R> q_mul_nd_add(const Q<R>& s, const Q<R>&
 }
 
 template <typename R>
+__host__ __device__ __forceinline__ Q<R> q_mul_dn_add(const Q<R>& s, const Q<R>& a, const Q<R>& b)
+{
+    Q<R> r;
+    r.c0 = s.c0 + a.c0 * b.c0 + a.c1 * b.c1 + a.c2 * b.c2 + a.c3 * b.c3;
+    r.c1 = s.c1 + a.c0 * b.c1 - a.c1 * b.c0 + a.c2 * b.c3 - a.c3 * b.c2;
+    r.c2 = s.c2 + a.c0 * b.c2 - a.c1 * b.c3 - a.c2 * b.c0 + a.c3 * b.c1;
+    r.c3 = s.c3 + a.c0 * b.c3 + a.c1 * b.c2 - a.c2 * b.c1 - a.c3 * b.c0;
+    return r;
+}
+
+template <typename R>
 __host__ __device__ __forceinline__ Q<R> q_dag(const Q<R>& a) { return q_make<R>(a.c0, -a.c1, -a.c2, -a.c3); }
 
 template <typename R>

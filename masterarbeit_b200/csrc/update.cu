@@ -9,7 +9,8 @@
 // counterpart: U' = W^dag U^dag W^dag with W = A/|A|.
 //
 // Every updated link is reprojected before its store (in place of project_gfield_to_sun after
-// the sweep, update.c:166).  Randoms come from Philox keyed by (seed, site, sweep, dir, draw,
+// the sweep, update.c:166), except an FP64 heatbath draw, which is unit to rounding (hb_store).
+// Randoms come from Philox keyed by (seed, site, sweep, dir, draw,
 // replica), so the result does not depend on grid shape or on which thread takes which link.
 #include <cfloat>
 #include <cmath>
@@ -46,7 +47,7 @@ __global__ void __launch_bounds__(update_block<KIND>(), 1024 / update_block<KIND
             Q<R> out;
             uint32_t trials = 0;
             if (heatbath_link<R>(A, beta, seed, (uint32_t)s.n, sweep, (uint32_t)MU, replica, trials, out, status))
-                U.sth(MU, par, h, q_project(out));
+                U.sth(MU, par, h, hb_store(out));
             if (acc_sum && trials) acc_thread = 1.0 / (double)trials;
         } else {
             U.sth(MU, par, h, q_project(overrelax_link<R>(A, U.ldh(MU, par, h))));
@@ -100,7 +101,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_visit(Field<R> U, Geom g, int par
                     }
                     if (trials) acc_thread += 1.0 / (double)trials;
                 }
-                if (changed) U.sth(MU, par, h, q_project(cur));
+                if (changed) U.sth(MU, par, h, hb_store(cur));
             } else {
                 uint32_t accepted = 0;
                 const Q<R> u = metropolis_link<R>(A, U.ldh(MU, par, h), (R)a.beta, (R)a.eps, visits * a.hits, a.seed,
