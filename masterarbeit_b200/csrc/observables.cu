@@ -264,14 +264,16 @@ __device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g,
     const Q<R> UT = U.ld(0, par, n);
     int tn = t + 1;
     tn -= tn >= g.L[0] ? g.L[0] : 0;
-    const size_t up = (size_t)(tn * sw + j) * RC, own = (size_t)threadIdx.x * RC;
+    // buffer layout [T & 1][r][thread]: a warp's 16-byte accesses to one r are consecutive, so they
+    // are free of bank conflicts (a per-thread block of RC loops put lanes RC * 16 bytes apart)
+    const int up = tn * sw + j, nt = blockDim.x;
     for (int T = 1; T <= thi; ++T) {
-        Q<R>* buf = ybuf + (size_t)(T & 1) * blockDim.x * RC;
+        Q<R>* buf = ybuf + (size_t)(T & 1) * nt * RC;
 #pragma unroll
-        for (int r = 0; r < RC; ++r) buf[own + r] = Y[r];
+        for (int r = 0; r < RC; ++r) buf[(size_t)r * nt + threadIdx.x] = Y[r];
         __syncthreads();   // the other buffer was last read before the previous barrier
 #pragma unroll
-        for (int r = 0; r < RC; ++r) Y[r] = q_mul_nd(q_mul(UT, buf[up + r]), UR[r]);
+        for (int r = 0; r < RC; ++r) Y[r] = q_mul_nd(q_mul(UT, buf[(size_t)r * nt + up]), UR[r]);
         if (T < tlo) continue;
 #pragma unroll
         for (int r = 0; r < RC; ++r) {
@@ -570,11 +572,12 @@ template <typename R, int RC>
 void wilson_smem_attr(int bytes)
 {
     cudaFuncSetAttribute(k_wilson_col<R, RC>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    // the small FP32 CTAs need ~45 KB for five per SM; without a preference the driver picked a
-    // 32 KB carveout.  The other instances keep the default, which leaves L1 its room (a maximal
+    // the small FP32 CTAs (96 threads, two buffers of RC loops, ~13 KB) fit six per SM by their
+    // registers and need ~80 KB of shared memory for that; without a preference the driver picked a
+    // 32 KB carveout.  The FP64 instances keep the default, which leaves L1 its room (a maximal
     // carveout cost FP64 5 %).
     if (sizeof(R) == 4 && RC >= 4)
-        cudaFuncSetAttribute(k_wilson_col<R, RC>, cudaFuncAttributePreferredSharedMemoryCarveout, 25);
+        cudaFuncSetAttribute(k_wilson_col<R, RC>, cudaFuncAttributePreferredSharedMemoryCarveout, 50);
 }
 
 }  // namespace
