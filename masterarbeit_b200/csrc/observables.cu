@@ -211,11 +211,6 @@ constexpr int kWilsonColMaxThreads = 512;
 template <typename R>
 __host__ __device__ constexpr bool wilson_thread_slots() { return sizeof(R) == 8; }
 
-// Quaternions of shared memory per thread and R in the column kernel: FP32 transports the loops
-// through two buffers, FP64 keeps one array of spatial lines.
-template <typename R>
-__host__ __device__ constexpr int wilson_col_bufs() { return sizeof(R) == 4 ? 2 : 1; }
-
 template <typename R>
 __device__ __forceinline__ size_t wilson_slot(int r, int ti, int nT, int warp)
 {
@@ -284,62 +279,14 @@ __device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g,
     __syncthreads();   // the buffers are written again by the next direction
 }
 
-// FP64 form of the column sums: the temporal lines T_T(x) and T_T(x + R k) are built up per T and
-// the spatial line S_R(x + T t) is read from the shared-memory line array of the thread one T up
-// (the transported form above needs three RC-loop registers more, which spill in FP64).
-template <typename R, int K, int RC>
-__device__ __forceinline__ void wilson_col_dir_lines(const Field<R>& U, const Geom& g, Q<R>* __restrict__ line,
-                                               double* __restrict__ wacc, int sw, int t, int j, int s, bool valid,
-                                               int r0, int tlo, int thi)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nT = thi - tlo + 1;
-    int par;
-    const int n = t * g.S[0] + s;
-    const Site st = site_lex(g, n, par);
-    Q<R>* own = line + (size_t)threadIdx.x * RC;
-    int xr[RC];    // lexicographic index of x + (r0 + r) k
-    Q<R> SX[RC];   // the thread's own spatial lines, kept in registers across the T loop
-    Q<R> S = q_one<R>();
-    for (int jj = 0; jj < r0 - 1; ++jj) S = q_mul(S, U.ld(K, par ^ (jj & 1), n + shift_k<K>(g, st.c[K], jj)));
-#pragma unroll
-    for (int r = 0; r < RC; ++r) {
-        const int jj = r0 - 1 + r;
-        S = q_mul(S, U.ld(K, par ^ (jj & 1), n + shift_k<K>(g, st.c[K], jj)));
-        own[r] = S;
-        SX[r] = S;
-        xr[r] = n + shift_k<K>(g, st.c[K], jj + 1);
-    }
-    __syncthreads();
-    Q<R> TX = q_one<R>(), TR[RC];
-#pragma unroll
-    for (int r = 0; r < RC; ++r) TR[r] = q_one<R>();
-    for (int T = 1; T <= thi; ++T) {
-        const int tprev = shift_t(g, st.c[0], T - 1);
-        const int pprev = par ^ ((T - 1) & 1);
-        TX = q_mul(TX, U.ld(0, pprev, n + tprev));
-#pragma unroll
-        for (int r = 0; r < RC; ++r) TR[r] = q_mul(TR[r], U.ld(0, pprev ^ ((r0 + r) & 1), xr[r] + tprev));
-        if (T < tlo) continue;
-        int tt = t + T;
-        if (tt >= g.L[0]) tt -= g.L[0];
-        const Q<R>* other = line + (size_t)(tt * sw + j) * RC;   // S_{r0+r}(x + T t)
-#pragma unroll
-        for (int r = 0; r < RC; ++r) {
-            const R w = valid ? q_dot(q_mul(TX, other[r]), q_mul(SX[r], TR[r])) : R(0);
-            wilson_acc<R>(wacc, w, wilson_slot<R>(r, T - tlo, nT, warp), lane);
-        }
-    }
-    __syncthreads();   // `line` is overwritten next
-}
-
 template <typename R, int RC>
 __global__ void __launch_bounds__(kWilsonColMaxThreads, 1) k_wilson_col(Field<R> U, Geom g, int sw, int r0, int tlo,
                                                                         int thi, DD* __restrict__ partials)
 {
     extern __shared__ __align__(16) unsigned char wsm[];
-    Q<R>* ybuf = (Q<R>*)wsm;   // FP32: two buffers of RC loops per thread; FP64: RC spatial lines
+    Q<R>* ybuf = (Q<R>*)wsm;   // two buffers of RC loops per thread
     const int nwarps = blockDim.x >> 5, nT = thi - tlo + 1;
-    double* wacc = (double*)(wsm + (size_t)wilson_col_bufs<R>() * blockDim.x * RC * sizeof(Q<R>));
+    double* wacc = (double*)(wsm + (size_t)2 * blockDim.x * RC * sizeof(Q<R>));
     const int owners = wilson_thread_slots<R>() ? (int)blockDim.x : nwarps;
     for (int i = threadIdx.x; i < owners * RC * nT; i += blockDim.x) wacc[i] = 0.0;
     __syncthreads();
@@ -349,12 +296,9 @@ __global__ void __launch_bounds__(kWilsonColMaxThreads, 1) k_wilson_col(Field<R>
         const int s_req = tile * sw + j;
         const bool valid = s_req < stot;
         const int s = valid ? s_req : stot - 1;   // threads past the end read a valid site and add 0
-        if (sizeof(R) == 4) wilson_col_dir<R, 1, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
-        else wilson_col_dir_lines<R, 1, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
-        if (sizeof(R) == 4) wilson_col_dir<R, 2, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
-        else wilson_col_dir_lines<R, 2, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
-        if (sizeof(R) == 4) wilson_col_dir<R, 3, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
-        else wilson_col_dir_lines<R, 3, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
+        wilson_col_dir<R, 1, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
+        wilson_col_dir<R, 2, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
+        wilson_col_dir<R, 3, RC>(U, g, ybuf, wacc, sw, t, j, s, valid, r0, tlo, thi);
     }
     // fixed-order sum over warps; slot r * kWilsonTChunk + (T - tlo) as in k_wilson
     for (int i = threadIdx.x; i < RC * nT; i += blockDim.x) {
@@ -390,7 +334,7 @@ template <typename R, int RC>
 size_t wilson_col_smem(int threads, int nT)
 {
     const int owners = wilson_thread_slots<R>() ? threads : threads / 32;
-    return (size_t)wilson_col_bufs<R>() * threads * RC * sizeof(Q<R>) + (size_t)owners * RC * nT * sizeof(double);
+    return (size_t)2 * threads * RC * sizeof(Q<R>) + (size_t)owners * RC * nT * sizeof(double);
 }
 
 // --------------------------------------------------- topological charge ---
@@ -726,9 +670,10 @@ int su2g::wilson_enqueue(su2g_lattice* h, void* const dirs[4], const int32_t* R,
     std::vector<Chunk> plan;
     std::vector<int> slot_rt((size_t)rmax * tmax, -1);
     int used = 0;
-    // the column kernel reads the lines at x + T t instead of rebuilding them, so narrow R chunks
-    // cost it little, and 4 keeps it at two CTAs per SM; the per-site kernel prefers 8
-    const int rc_max = wilson_col_width(h->g) > 0 ? 4 : 8;
+    // the column kernel transports its loops in time, so a narrow R chunk costs it only the rebuild
+    // of its spatial lines: FP32 runs chunks of 4 loops per thread, FP64 of 2 (4 spills in FP64:
+    // 22.5 ms against 11.2 ms for W(R, T <= 9) at 48^4); the per-site kernel prefers 8
+    const int rc_max = wilson_col_width(h->g) > 0 ? (h->prec == SU2G_FP32 ? 4 : 2) : 8;
     for (int r0 = 1; r0 <= rmax;) {
         const int left = rmax - r0 + 1;
         const int rc_n = left >= 8 && rc_max >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
