@@ -40,6 +40,7 @@ FALLBACK_HBM_GBS = 6650.0
 
 R9 = [r for r in range(1, 10) for t in range(1, 10)]
 T9 = [t for r in range(1, 10) for t in range(1, 10)]
+APE_SEQ = 10   # smearing steps per timed call
 # one call of each kernel family on a lattice L (the --kernel mode)
 KERNELS = {
     "heatbath": lambda L: L.sweep(1, 1, 0),
@@ -480,10 +481,12 @@ def precision_figures(L, prec, dims, K, W, peak, clk, extras):
     hb = lambda: (L.sweep(1, 1, 0), L.plaquette())
     ms = time_steps(L, K, hb)
     extras[f"{prec}_heatbath_link_updates_per_s"] = 4 * vol * K / (ms / 1e3)
+    # smearing runs in sequences (15 / 30 APE_all steps before Q, 100-400 spatial before W): each
+    # figure is per step within sequences of APE_SEQ steps
     for mode, per_site in (("all", 8), ("spatial", 6)):
-        L.ape(1, 0.5, mode)
-        rate, gbs, frac = kernel_rate(L, K, lambda: L.ape(1, 0.5, mode), "ape", vol, per_site * lb, peak)
-        extras[f"{prec}_ape_{mode}_steps_per_s"] = rate
+        L.ape(APE_SEQ, 0.5, mode)
+        rate, gbs, frac = kernel_rate(L, K, lambda: L.ape(APE_SEQ, 0.5, mode), "ape", vol, per_site * lb, peak)
+        extras[f"{prec}_ape_{mode}_steps_per_s"] = rate * APE_SEQ
         extras[f"{prec}_ape_{mode}_gbs"] = gbs
         extras[f"{prec}_ape_{mode}_frac_of_peak"] = frac
     R = [r for r in range(1, 10) for t in range(1, 10)]
@@ -564,9 +567,9 @@ def big_lattice_figures(device, seed, K=3):
         ms = time_steps(L, K, lambda: L.sweep(1, 1, N_OR))
         out[f"{prec}_1hb{N_OR}or_link_updates_per_s"] = (1 + N_OR) * 4 * vol * K / (ms / 1e3)
         for mode in ("all", "spatial"):
-            L.ape(1, 0.5, mode)
-            ms = time_steps(L, K, lambda: L.ape(1, 0.5, mode))
-            out[f"{prec}_ape_{mode}_steps_per_s"] = K / (ms / 1e3)
+            L.ape(APE_SEQ, 0.5, mode)
+            ms = time_steps(L, K, lambda: L.ape(APE_SEQ, 0.5, mode))
+            out[f"{prec}_ape_{mode}_steps_per_s"] = APE_SEQ * K / (ms / 1e3)
         if prec == "fp32":
             R = [r for r in range(1, 13) for t in range(1, 21)]
             T = [t for r in range(1, 13) for t in range(1, 21)]

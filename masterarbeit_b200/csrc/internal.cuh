@@ -193,6 +193,9 @@ namespace su2g {
 int ape_enqueue(su2g_lattice* h, int ns, double alpha, int mode);
 // One smearing step from the field at in_dirs into out_dirs (only the smeared directions are written).
 int ape_step(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], int mode, double alpha);
+// `steps` smearing steps on (cur, alt); the smeared directions swap buffers after every step, so
+// the result is at cur.
+int ape_run(su2g_lattice* h, void* cur[4], void* alt[4], int steps, int mode, double alpha);
 // TMA-tiled APE_all (FP32): rows per CTA if it applies to the geometry, else 0; and its launch.
 int ape_tma_rows(const Geom& g, int max_smem);
 int ape_tma_launch(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs[4], double alpha, int yb);

@@ -61,20 +61,6 @@ int copy_field(su2g_lattice* h, void* const dst[4])
     return SU2G_OK;
 }
 
-// `steps` smearing steps on (cur, alt); the smeared directions swap buffers after every step.
-int smear(su2g_lattice* h, void* cur[4], void* alt[4], int steps, int mode, double alpha)
-{
-    for (int s = 0; s < steps; ++s) {
-        int rc = ape_step(h, cur, alt, mode, alpha);
-        if (rc) return rc;
-        for (int mu = 0; mu < 4; ++mu) {
-            const bool upd = mode == SU2G_APE_ALL || (mode == SU2G_APE_SPATIAL ? mu != 0 : mu == 0);
-            if (upd) std::swap(cur[mu], alt[mu]);
-        }
-    }
-    return SU2G_OK;
-}
-
 int enqueue_measurement(su2g_lattice* h, su2g_meas_graph& m)
 {
     int rc = SU2G_OK;
@@ -86,7 +72,7 @@ int enqueue_measurement(su2g_lattice* h, su2g_meas_graph& m)
         if ((rc = copy_field(h, cur))) return rc;
         int done = 0;
         for (int i = 0; i < nq; ++i) {
-            if ((rc = smear(h, cur, alt, m.q_ape[i] - done, SU2G_APE_ALL, m.alpha_q))) return rc;
+            if ((rc = ape_run(h, cur, alt, m.q_ape[i] - done, SU2G_APE_ALL, m.alpha_q))) return rc;
             done = m.q_ape[i];
             // Q and sum |q| into d_out[2i], d_out[2i + 1]
             if ((rc = qtop_enqueue(h, cur, 2 * i))) return rc;
@@ -96,8 +82,8 @@ int enqueue_measurement(su2g_lattice* h, su2g_meas_graph& m)
         work_dirs(h, h->meas_work, cur);
         work_dirs(h, h->meas_alt, alt);
         if ((rc = copy_field(h, cur))) return rc;
-        if ((rc = smear(h, cur, alt, m.ns_t, SU2G_APE_TEMPORAL, m.alpha_t))) return rc;
-        if ((rc = smear(h, cur, alt, m.ns_s, SU2G_APE_SPATIAL, m.alpha_s))) return rc;
+        if ((rc = ape_run(h, cur, alt, m.ns_t, SU2G_APE_TEMPORAL, m.alpha_t))) return rc;
+        if ((rc = ape_run(h, cur, alt, m.ns_s, SU2G_APE_SPATIAL, m.alpha_s))) return rc;
         m.wslot.assign(nw, 0);
         const int off = 2 * nq;
         if ((rc = wilson_enqueue(h, cur, m.R.data(), m.T.data(), nw, off, kOutSlots - 2 - off, m.wslot.data())))

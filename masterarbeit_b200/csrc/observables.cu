@@ -570,16 +570,21 @@ int su2g::ape_step(su2g_lattice* h, void* const in_dirs[4], void* const out_dirs
     return launch_end(h, SU2G_K_APE, "APE kernel");
 }
 
-int su2g::ape_enqueue(su2g_lattice* h, int ns, double alpha, int mode)
+int su2g::ape_run(su2g_lattice* h, void* cur[4], void* alt[4], int steps, int mode, double alpha)
 {
-    int rc = ensure_alt(h);
-    if (rc) return rc;
-    for (int step = 0; step < ns; ++step) {
-        if ((rc = ape_step(h, h->dirp, h->altp, mode, alpha))) return rc;
+    for (int step = 0; step < steps; ++step) {
+        const int rc = ape_step(h, cur, alt, mode, alpha);
+        if (rc) return rc;
         for (int mu = 0; mu < 4; ++mu)
-            if (ape_updates(mode, mu)) std::swap(h->dirp[mu], h->altp[mu]);
+            if (ape_updates(mode, mu)) std::swap(cur[mu], alt[mu]);
     }
     return SU2G_OK;
+}
+
+int su2g::ape_enqueue(su2g_lattice* h, int ns, double alpha, int mode)
+{
+    const int rc = ensure_alt(h);
+    return rc ? rc : ape_run(h, h->dirp, h->altp, ns, mode, alpha);
 }
 
 int su2g::ensure_lines(su2g_lattice* h)

@@ -16,6 +16,7 @@ def test_tma_ape_matches_generic_and_oracle(dims):
     tma = Lattice(dims, precision="fp32", seed=17, start="haar")
     gen = Lattice(dims, precision="fp32", seed=17, start="haar")
     tma.set_kernel_variant("ape", 1)
+    gen.set_kernel_variant("ape", 0)
     assert tma.kernel_variant("ape") == 1 and gen.kernel_variant("ape") == 0
     U = tma.download()
     tma.ape(3, 0.5, "all")
