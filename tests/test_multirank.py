@@ -60,3 +60,91 @@ def test_reference_arm_under_two_ranks():
     line = lines[0]
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "reference"
+
+
+FAKE_ARM = r'''
+import json, os, sys
+sys.path.insert(0, REPO)
+import bench
+import masterarbeit_b200.su2g as S
+
+RANK = int(os.environ["RANK"])
+
+
+class FakeLattice:
+    """Host stand-in for a GPU lattice: every timed block of calls takes (5 + rank) ms, and the
+    profiled pass reports one event-timed launch per call and kernel class."""
+
+    def __init__(self, dims, **kw):
+        self.calls = {"heatbath": 0, "plaquette": 0}
+        self.profiling = False
+
+    def sweep(self, n_sweeps=1, n_hb=1, n_or=0, acc=False):
+        self.calls["heatbath"] += 8 * n_sweeps
+
+    def plaquette(self):
+        self.calls["plaquette"] += 1
+        return 0.5
+
+    def synchronize(self):
+        pass
+
+    def timer_begin(self):
+        pass
+
+    def timer_end(self):
+        return 5.0 + RANK
+
+    def profile(self, on=True):
+        self.profiling = on
+        self.calls = {k: 0 for k in self.calls}
+
+    def profile_read(self):
+        return {k: (n, 0.1 * n) for k, n in self.calls.items()}
+
+    def download(self, out=None):
+        return out
+
+    def upload(self, links):
+        pass
+
+    def close(self):
+        pass
+
+
+class FakePinned:
+    def __init__(self, shape, dtype=None):
+        self.array = None
+
+    def free(self):
+        pass
+
+
+S.Lattice, S.PinnedArray = FakeLattice, FakePinned
+sys.argv = ["bench.py", "--gpus", "2", "--steps", "4", "--warmup", "3", "--no-extras", "--no-cpu", "--dims", "8,8,8,8"]
+args = bench.parse()
+d = bench.Dist()
+bench.run_ours(args, d, [8, 8, 8, 8])
+d.close()
+'''
+
+
+def test_repo_arm_rank_plumbing_under_two_ranks(tmp_path):
+    """bench.py's own arm under torchrun with two gloo ranks, the lattice replaced by a host fake:
+    rank 0 alone prints one line, timed as the maximum over ranks, with the whole-job aggregate."""
+    script = tmp_path / "arm.py"
+    script.write_text(f"REPO = {O.REPO!r}\n" + FAKE_ARM)
+    r = _torchrun([str(script)])
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    line = lines[0]
+    vol, K = 8 ** 4, 4
+    # the slower rank (rank 1: 6 ms for the K steps) sets the job's time
+    assert line["n_gpus"] == 2 and line["steps"] == K and line["warmup"] == 3
+    assert line["ms_per_step"] == 6.0 / K
+    assert abs(line["value"] - 4 * vol * K * 2 / 6e-3) <= 1e-6 * line["value"]
+    assert abs(line["e2e"]["value"] - 4 * vol * K * 2 / 6e-3) <= 1e-6 * line["value"]
+    assert line["scaling"] == "weak" and line["config"]["parallelism"] == "replicas x2"
+    assert line["roofline"]["launches"] == 8 * K and line["gpu_launches"] == 9 * K
+    assert "cpu_baseline" not in line   # rank 0 at N = 1 only
