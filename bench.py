@@ -399,13 +399,11 @@ def batch_figures(dist, sweeps=1000, seq_sweeps=20):
         Ls = [Lattice(r["dims"], precision="fp32", beta=r["beta"], seed=r["seed"], start=r["start"],
                       replica=r["replica"], device=dist.local) for r in reps]
         for L in Ls:
-            L.sweep(1, 1, N_OR)
-            L.plaquette()
+            L.sweep_plaquette(1, 1, N_OR)
         t0 = time.perf_counter()
         for _ in range(seq_sweeps):
             for L in Ls:
-                L.sweep(1, 1, N_OR)
-                L.plaquette()
+                L.sweep_plaquette(1, 1, N_OR)
         ms_sweep_seq = (time.perf_counter() - t0) * 1e3 / seq_sweeps
         for L in Ls:
             L.close()
@@ -428,20 +426,19 @@ def graph_figures(dist, sweeps=200):
     for prec in ("fp64", "fp32"):
         a = Lattice((8, 8, 8, 8), precision=prec, beta=3.09, seed=1, start="cold", device=dist.local)
         b = Lattice((8, 8, 8, 8), precision=prec, beta=3.09, seed=1, start="cold", device=dist.local)
-        a.sweep(5, 1, N_OR)
-        a.plaquette()
+        for _ in range(5):
+            a.sweep_plaquette(1, 1, N_OR)
         b.graph_run(5, 1, 1, N_OR)
         t0 = time.perf_counter()
         for _ in range(sweeps):
-            a.sweep(1, 1, N_OR)
-            a.plaquette()
+            p_last = a.sweep_plaquette(1, 1, N_OR)
         plain = time.perf_counter() - t0
         t0 = time.perf_counter()
         trace, _ = b.graph_run(sweeps, 1, 1, N_OR)
         graph = time.perf_counter() - t0
         out[f"{prec}_8x8x8x8"] = {"sweeps": sweeps, "plain_sweeps_per_s": sweeps / plain,
                                   "graph_sweeps_per_s": sweeps / graph, "speedup": plain / graph,
-                                  "identical_to_plain": bool(abs(trace[-1] - a.plaquette()) == 0.0)}
+                                  "identical_to_plain": bool(trace[-1] == p_last)}
         a.close()
         b.close()
     return out
@@ -464,7 +461,7 @@ def precision_figures(L, prec, dims, K, W, peak, clk, extras):
     the heatbath-only sweep, APE all / spatial, W(R<=9, T<=9) and Q."""
     vol = math.prod(dims)
     lb = 16 if prec == "fp32" else 32
-    step = lambda: (L.sweep(1, 1, N_OR), L.plaquette())
+    step = lambda: L.sweep_plaquette(1, 1, N_OR)
     for _ in range(W):
         step()
     ms = time_steps(L, K, step)
@@ -478,7 +475,7 @@ def precision_figures(L, prec, dims, K, W, peak, clk, extras):
         gbs = (vol // 2) * transfers * lb / (tms / n / 1e3) / 1e9
         extras[f"{prec}_{cls}_pass_gbs"] = gbs
         extras[f"{prec}_{cls}_pass_frac_of_peak"] = gbs / peak
-    hb = lambda: (L.sweep(1, 1, 0), L.plaquette())
+    hb = lambda: L.sweep_plaquette(1, 1, 0)
     ms = time_steps(L, K, hb)
     extras[f"{prec}_heatbath_link_updates_per_s"] = 4 * vol * K / (ms / 1e3)
     # smearing runs in sequences (15 / 30 APE_all steps before Q, 100-400 spatial before W): each
@@ -599,9 +596,8 @@ def run_ours(args, dist, dims):
     # heatbath sweep of all 4V links, then the plaquette (qcd.c:54-60: gaugefieldUpdate, plaquette)
     lat = Lattice(dims, precision="fp64", beta=BETA, seed=1000 + rank, start="haar", replica=rank, device=dist.local)
 
-    def step():
-        lat.sweep(1, 1, 0)
-        lat.plaquette()
+    def step():   # su2g_sweep_plaquette: the plaquette is summed inside the sweep's last update passes
+        lat.sweep_plaquette(1, 1, 0)
 
     for _ in range(W):
         step()
@@ -633,12 +629,13 @@ def run_ours(args, dist, dims):
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic: Philox Haar-random hot start (no checkpoints or datasets)",
         "config": {"workload": f"{'x'.join(map(str, dims))} SU(2) beta={BETA} hot start; step = 1 checkerboard "
-                               "heatbath sweep (heatbath only, as the reference) + plaquette",
+                               "heatbath sweep (heatbath only, as the reference) + plaquette (summed inside "
+                               "the sweep's last update passes)",
                    "dims": list(dims), "precision": "fp64 links and arithmetic, as the reference",
                    "l2": f"inputs larger than L2 (field {4 * vol * link64 / 1e6:.0f} MB > 126 MB)",
                    "parallelism": f"replicas x{dist.world}"},
-        "roofline": {"bound": "hbm", "kernel": "FP64 heatbath pass k_update<double, mu, 0> (8 of the 8 update "
-                                              "launches of a step)",
+        "roofline": {"bound": "hbm", "kernel": "FP64 heatbath pass k_update<double, mu, 0> (the 8 update "
+                                              "launches of a step; 3 of them also sum the plaquette)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6650 GB/s",
@@ -697,8 +694,7 @@ def run_ours(args, dist, dims):
 
     def e2e_step():
         lat.upload(host.array)
-        lat.sweep(1, 1, 0, acc=True)
-        lat.plaquette()
+        lat.sweep_plaquette(1, 1, 0, acc=True)
 
     e2e_step()
     dist.barrier()
@@ -710,7 +706,7 @@ def run_ours(args, dist, dims):
                    "h2d_bytes_per_step": vol * 16 * 8, "d2h_bytes_per_step": 8 + 8,
                    "host_wall_s": wall_e2e,
                    "what": "su2g_upload_aos_f64 (pinned host FP64 field, the reference's pu block) + "
-                           "su2g_sweep(1 heatbath, acceptance read back) + su2g_plaquette (read back)"}
+                           "su2g_sweep_plaquette(1 heatbath sweep; plaquette and acceptance read back)"}
     host.free()
 
     if rank == 0 and dist.world == 1 and not args.no_cpu:

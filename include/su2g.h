@@ -98,6 +98,17 @@ int su2g_download_aos_f64(su2g_lattice *h, double *links);
  * receives the mean of 1/trials over all heatbath link updates (the `acc=` log value,
  * update.c:169-173) and the call synchronises; otherwise the call only enqueues. */
 int su2g_sweep(su2g_lattice *h, int32_t n_sweeps, int32_t n_hb, int32_t n_or, double *acc_out);
+/* su2g_sweep followed by plaquette() (plaquette.c:67-100) -- the qcd.c:55-60 loop body -- with the
+ * plaquette summed inside the update passes: in the parity-1 passes of mu = 1, 2, 3 of the last
+ * sub-sweep, (U'_mu(x) A_low(x)).c0 over the odd sites, A_low the staple terms of the planes
+ * (mu, nu < mu), covers all 6V plaquettes of the final field once (each holds one odd-site link of
+ * its higher direction, and the plaquette's other links are final by then).  *plaq equals
+ * su2g_plaquette of the resulting field to rounding (the terms are summed in another order).  The
+ * field and the acceptance equal su2g_sweep's to rounding: the fused passes are separately compiled
+ * kernels whose multiply-adds may round differently in the last bit.  Synchronises.  With no
+ * sub-sweep, *plaq is su2g_plaquette. */
+int su2g_sweep_plaquette(su2g_lattice *h, int32_t n_sweeps, int32_t n_hb, int32_t n_or, double *plaq,
+                         double *acc_out);
 
 /* gaugefieldUpdate(iup, nup, utype, stype) with both of the reference's update algorithms and
  * sweep orders (update.c:102-175).  utype 1 = heatbath, 0 = Metropolis: localMetropolisUpdate
@@ -184,7 +195,7 @@ int su2g_stats_veff(const double *w, int32_t n_conf, int32_t n_r, int32_t n_t, i
  * replayed CUDA graph.  Runs n_blocks blocks of [meas_every x (n_hb heatbath + n_or overrelaxation
  * sweeps), plaquette].  The block is captured on first use and replayed; it is captured again
  * when the block shape, beta, the seed or the field's buffers have changed.  The results equal
- * those of the same su2g_sweep / su2g_plaquette sequence bit for bit.  plaq[b] and acc[b] (either
+ * those of the same su2g_sweep_plaquette sequence bit for bit.  plaq[b] and acc[b] (either
  * may be NULL) receive the plaquette after block b and block b's mean heatbath acceptance. */
 int su2g_graph_run(su2g_lattice *h, int32_t n_blocks, int32_t meas_every, int32_t n_hb, int32_t n_or,
                    double *plaq, double *acc);

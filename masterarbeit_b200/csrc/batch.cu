@@ -325,7 +325,7 @@ __device__ __forceinline__ void persist_pass(const PersistArgs& a, const int* __
         const int h = gi - s_pre[lo];
         const FieldCG<R> U = rep_field_cg<R>(rp);
         const Site s = site_of(g, par, h);
-        const Q<R> A = staple_update<R, MU, FieldCG<R>>(U, g, s, par);
+        const Q<R> A = staple_update<R, MU, 0, FieldCG<R>>(U, g, s, par);
         if (KIND == SU2G_HEATBATH) {
             Q<R> out;
             uint32_t trials = 0;

@@ -144,12 +144,62 @@ __global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const DD* __restric
     if (threadIdx.x == 0) out[blockIdx.x] = (v.s + v.e) * scale;
 }
 
+// One slot of many partials: CTA b sums the contiguous chunk b (fixed assignment), and the CTA
+// that arrives last on the counter sums the CTA results in index order and clears the counter, so
+// the result does not depend on which CTA finished when.  (The fused plaquette's 249k partials
+// at 48^4 took 17 us in one CTA of k_finalize.)
+constexpr int kFinWideThreads = 256;
+static_assert(kFinBlocks <= kFinWideThreads, "the last CTA sums one CTA result per thread");
+
+__global__ void __launch_bounds__(kFinWideThreads) k_finalize_wide(const DD* __restrict__ partials, int nparts,
+                                                                   double scale, double* __restrict__ out,
+                                                                   DD* __restrict__ blocks, unsigned* ticket)
+{
+    const int nb = gridDim.x;
+    const int chunk = (nparts + nb - 1) / nb;
+    const int lo = blockIdx.x * chunk, hi = min(nparts, lo + chunk);
+    DD acc[2] = {{0.0, 0.0}, {0.0, 0.0}};
+    int i = lo + threadIdx.x;
+    for (; i + kFinWideThreads < hi; i += 2 * kFinWideThreads) {
+        acc[0] = dd_add(acc[0], partials[i]);
+        acc[1] = dd_add(acc[1], partials[i + kFinWideThreads]);
+    }
+    if (i < hi) acc[0] = dd_add(acc[0], partials[i]);
+    const DD v = dd_block_sum<kFinWideThreads>(dd_add(acc[0], acc[1]));
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        blocks[blockIdx.x] = v;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == (unsigned)nb - 1u;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    DD w = {0.0, 0.0};
+    if (threadIdx.x < nb) {
+        const double2 b = __ldcg(reinterpret_cast<const double2*>(blocks) + threadIdx.x);
+        w.s = b.x;
+        w.e = b.y;
+    }
+    w = dd_block_sum<kFinWideThreads>(w);
+    if (threadIdx.x == 0) {
+        *out = (w.s + w.e) * scale;
+        *ticket = 0u;
+    }
+}
+
 int finalize(su2g_lattice* h, int nparts, int nslots, double scale, int out_off, int stride)
 {
     if (out_off + nslots > kOutSlots) return set_error(h, SU2G_EINVAL, "too many result slots");
     launch_begin(h, SU2G_K_REDUCE);
-    k_finalize<<<nslots, kFinalizeBlock, 0, h->stream>>>(h->partials, nparts, stride > 0 ? stride : kMaxPartials,
-                                                          scale, h->d_out + out_off);
+    if (nslots == 1 && nparts > 4 * kFinalizeBlock) {
+        const int nb = std::min(kFinBlocks, (nparts + 2 * kFinWideThreads - 1) / (2 * kFinWideThreads));
+        k_finalize_wide<<<nb, kFinWideThreads, 0, h->stream>>>(h->partials, nparts, scale, h->d_out + out_off,
+                                                              h->fin_blocks, h->fin_ticket);
+    } else {
+        k_finalize<<<nslots, kFinalizeBlock, 0, h->stream>>>(h->partials, nparts, stride > 0 ? stride : kMaxPartials,
+                                                              scale, h->d_out + out_off);
+    }
     return launch_end(h, SU2G_K_REDUCE, "finalize reduction");
 }
 
@@ -379,6 +429,11 @@ extern "C" int su2g_create(const su2g_params* p, su2g_lattice** out)
     if (!rc && (e = cudaMalloc(&h->d_status, sizeof(unsigned))) != cudaSuccess)
         rc = check_cuda(h, e, "allocating status word");
     if (!rc) rc = check_cuda(h, cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream), "clearing status");
+    if (!rc && (e = cudaMalloc(&h->fin_blocks, kFinBlocks * sizeof(DD))) != cudaSuccess)
+        rc = check_cuda(h, e, "allocating reduction scratch");
+    if (!rc && (e = cudaMalloc(&h->fin_ticket, sizeof(unsigned))) != cudaSuccess)
+        rc = check_cuda(h, e, "allocating reduction scratch");
+    if (!rc) rc = check_cuda(h, cudaMemsetAsync(h->fin_ticket, 0, sizeof(unsigned), h->stream), "clearing reduction counter");
     if (!rc) rc = ensure_partials(h, 2);
     if (!rc) wilson_prepare(h);
     if (!rc) rc = check_cuda(h, cudaEventCreate(&h->ev_begin), "creating events");
@@ -419,6 +474,8 @@ extern "C" int su2g_destroy(su2g_lattice* h)
     cudaFree(h->partials);
     cudaFree(h->d_out);
     cudaFree(h->d_status);
+    cudaFree(h->fin_blocks);
+    cudaFree(h->fin_ticket);
     cudaFree(h->d_aos);
     if (h->h_out) cudaFreeHost(h->h_out);
     if (h->stream) cudaStreamDestroy(h->stream);

@@ -13,6 +13,7 @@ namespace su2g {
 
 constexpr int kBlock = 256;            // threads per CTA for the stencil kernels
 constexpr int kMaxPartials = 8192;     // per-CTA partial sums a reduction may write
+constexpr int kFinBlocks = 128;        // CTAs of the wide final reduction (one slot, many partials)
 constexpr int kOutSlots = 16384;       // device result doubles per handle
 constexpr uint32_t kMaxTrials = 1u << 20;   // Kennedy-Pendleton trials before a link gives up
 
@@ -124,6 +125,8 @@ struct su2g_lattice {
     double* d_out = nullptr;     // device result slots
     double* h_out = nullptr;     // pinned host mirror of d_out
     unsigned* d_status = nullptr;
+    su2g::DD* fin_blocks = nullptr;   // per-CTA sums of the wide final reduction (kFinBlocks)
+    unsigned* fin_ticket = nullptr;   // its arrival counter (zero between launches)
     double* d_aos = nullptr;     // device staging for AoS FP64 transfers
     size_t aos_sites = 0;        // sites the staging buffer holds
     cudaStream_t stream = nullptr;
@@ -228,7 +231,17 @@ int wilson_check(su2g_lattice* h, const int32_t* R, const int32_t* T, int n, con
 // Enqueue the plaquette of the current field into d_out[out_off].
 int plaquette_enqueue(su2g_lattice* h, int out_off);
 // One (mu, parity) update pass.  The heatbath sweep index is `sweep`, plus *sweep_base when
-// sweep_base is given (a device counter, so that a captured graph advances it by itself).
+// sweep_base is given (a device counter, so that a captured graph advances it by itself).  With
+// plaq_part (parity-1 passes of mu >= 1 only) the pass also writes one plaquette partial per CTA.
 int launch_update(su2g_lattice* h, int kind, int mu, int par, uint32_t sweep, double* acc_sum,
-                  const uint32_t* sweep_base = nullptr);
+                  const uint32_t* sweep_base = nullptr, DD* plaq_part = nullptr);
+// CTAs of an update pass (one link per thread), and the plaquette partials of a fused pass.
+int update_grid(const su2g_lattice* h);
+int update_plaq_parts(const su2g_lattice* h);
+// Enqueue n_sweeps x (n_hb heatbath + n_or overrelaxation sweeps); heatbath sub-sweep j (counted
+// from 0 within the call) has index sweep0 + j (+ *base).  With plaq_off >= 0 the last sub-sweep
+// also sums the plaquette of the final field into d_out[plaq_off] (the plaquette kernel runs
+// instead when there is no sub-sweep); partials[0 .. 3 * update_plaq_parts) are used.
+int sweep_enqueue(su2g_lattice* h, int n_sweeps, int n_hb, int n_or, uint32_t sweep0, const uint32_t* base,
+                  double* acc_dev, int plaq_off);
 }  // namespace su2g

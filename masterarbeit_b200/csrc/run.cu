@@ -2,10 +2,12 @@
 //
 // Reference: the driver loop of LGT_Code/main/qcd.c:55-60, gaugefieldUpdate (update.c:102-175)
 // followed by plaquette() (plaquette.c:67-100) after every sweep.  One block is `meas_every`
-// sweeps of (n_hb heatbath + n_or overrelaxation) and one plaquette.  The heatbath sweep index
-// that keys the Philox stream and the trace row are device counters that the graph advances
-// itself, so a replayed block draws exactly the randoms su2g_sweep draws for the same sweeps and
-// the trace equals the one of the plain su2g_sweep / su2g_plaquette sequence bit for bit.
+// sweeps of (n_hb heatbath + n_or overrelaxation) and the plaquette, summed inside the last
+// sweep's update passes.  The heatbath sweep index that keys the Philox stream and the trace row
+// are device counters that the graph advances itself, so a replayed block draws exactly the randoms
+// su2g_sweep draws for the same sweeps and the trace equals the one of the plain
+// su2g_sweep_plaquette sequence bit for bit.
+#include <algorithm>
 #include <vector>
 
 #include "internal.cuh"
@@ -47,19 +49,9 @@ bool graph_matches(const su2g_lattice* h, int meas_every, int n_hb, int n_or)
 int enqueue_block(su2g_lattice* h, int meas_every, int n_hb, int n_or)
 {
     double* acc = h->d_out + kSlotAcc;
-    int rc = SU2G_OK;
-    for (int s = 0; s < meas_every; ++s) {
-        for (int i = 0; i < n_hb; ++i)
-            for (int mu = 0; mu < 4; ++mu)
-                for (int par = 0; par < 2; ++par)
-                    if ((rc = launch_update(h, SU2G_HEATBATH, mu, par, (uint32_t)(s * n_hb + i), acc, h->d_run_ctr)))
-                        return rc;
-        for (int i = 0; i < n_or; ++i)
-            for (int mu = 0; mu < 4; ++mu)
-                for (int par = 0; par < 2; ++par)
-                    if ((rc = launch_update(h, SU2G_OVERRELAX, mu, par, 0u, nullptr))) return rc;
-    }
-    if ((rc = plaquette_enqueue(h, kSlotPlaq))) return rc;
+    // the plaquette is summed inside the last sub-sweep's update passes (su2g_sweep_plaquette)
+    int rc = sweep_enqueue(h, meas_every, n_hb, n_or, 0u, h->d_run_ctr, acc, kSlotPlaq);
+    if (rc) return rc;
     const double nupd = (double)meas_every * n_hb * 4.0 * (double)h->g.V;
     k_run_record<<<1, 1, 0, h->stream>>>(h->d_out + kSlotPlaq, acc, h->d_run_ctr, h->d_trace, (uint32_t)h->trace_rows,
                                          nupd > 0 ? 1.0 / nupd : 0.0, (uint32_t)(meas_every * n_hb));
@@ -70,7 +62,7 @@ int capture(su2g_lattice* h, int meas_every, int n_hb, int n_or)
 {
     release_run_graph(h);
     // everything the block allocates is allocated before the capture starts
-    int rc = ensure_partial_entries(h, 2 * (size_t)((h->g.Vh + kBlock - 1) / kBlock));
+    int rc = ensure_partial_entries(h, std::max(2 * (size_t)((h->g.Vh + kBlock - 1) / kBlock), 3 * (size_t)update_plaq_parts(h)));
     if (rc) return rc;
     const bool prof = h->profiling;
     h->profiling = false;   // no per-launch events inside the graph

@@ -30,18 +30,29 @@ namespace {
 template <int KIND>
 constexpr int update_block() { return 128; }
 
-template <typename R, int MU, int KIND>
+// PLQ: the pass also sums the plaquettes of the planes (MU, nu < MU) of the configuration it leaves
+// (one partial per warp into plaq_part).  Run in the parity-1 passes of MU = 1, 2, 3 of a
+// sweep's last sub-sweep, these are all 6V plaquettes of the final field, each once: when U_MU(x)
+// at the odd sites is updated, every other link of the plaquettes of the planes (MU, nu < MU) is
+// final (directions nu < MU and U_MU at the even sites were updated by earlier passes), and each
+// such plaquette holds exactly one odd-site U_MU link.  So with A_low the staple terms nu < MU,
+// (1/2) Re tr of those plaquettes summed is (U'_MU(x) A_low(x)).c0, for the staple convention of
+// staple_update (U A = the sum of the plaquettes through U); the separate plaquette kernel
+// (plaquette.c:67-100) then need not run.
+template <typename R, int MU, int KIND, bool PLQ = false>
 __global__ void __launch_bounds__(update_block<KIND>(), 1024 / update_block<KIND>()) k_update(Field<R> U, Geom g, int par, R beta, uint64_t seed, uint32_t sweep,
                                                    const uint32_t* __restrict__ sweep_base, uint32_t replica,
-                                                   double* __restrict__ acc_sum, unsigned* __restrict__ status)
+                                                   double* __restrict__ acc_sum, unsigned* __restrict__ status,
+                                                   DD* __restrict__ plaq_part = nullptr)
 {
     // one link per thread; CTAs are dispatched in index order, so the CTAs in flight cover a
     // contiguous window of the lattice and neighbours one t-slice away are still in L2
-    double acc_thread = 0.0;
+    double acc_thread = 0.0, plaq_thread = 0.0;
     const int h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h < g.Vh) {
         const Site s = site_of(g, par, h);
-        const Q<R> A = staple_update<R, MU>(U, g, s, par);
+        Q<R> low;
+        const Q<R> A = staple_update<R, MU, PLQ ? MU : 0>(U, g, s, par, PLQ ? &low : nullptr);
         if (KIND == SU2G_HEATBATH) {
             if (sweep_base) sweep += *sweep_base;
             Q<R> out;
@@ -52,11 +63,28 @@ __global__ void __launch_bounds__(update_block<KIND>(), 1024 / update_block<KIND
         } else {
             U.sth(MU, par, h, q_project(overrelax_link<R>(A, U.ldh(MU, par, h))));
         }
+        if constexpr (PLQ) {
+            // the link as stored (or kept, if the trial bound was hit), read back through L2, which
+            // sees this thread's own store; the update above is the same code as without PLQ, so
+            // both kernels compile it alike and leave the same field
+            FieldCG<R> Uc;
+            for (int d = 0; d < 4; ++d) Uc.p[d] = U.p[d];
+            Uc.Vh = U.Vh;
+            plaq_thread = (double)q_mul(Uc.ldh(MU, par, h), low).c0;
+        }
     }
     if (KIND == SU2G_HEATBATH && acc_sum) {
         DD v = {acc_thread, 0.0};
         v = dd_block_sum<update_block<KIND>()>(v);
         if (threadIdx.x == 0) atomicAdd(acc_sum, v.s + v.e);
+    }
+    if (PLQ) {
+        // one partial per warp (plain FP64 over its 32 terms), no CTA barrier: a barrier would
+        // hold the CTA's warps until its slowest Kennedy-Pendleton lane is done
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) plaq_thread += __shfl_xor_sync(0xffffffffu, plaq_thread, o);
+        if ((threadIdx.x & 31) == 0)
+            plaq_part[blockIdx.x * (update_block<KIND>() / 32) + (threadIdx.x >> 5)] = DD{plaq_thread, 0.0};
     }
 }
 
@@ -139,33 +167,56 @@ void launch_visit_r(su2g_lattice* h, int kind, int order, int mu, int par, const
 }
 
 template <typename R, int KIND>
-void launch_update_t(su2g_lattice* h, int mu, int par, uint32_t sweep, const uint32_t* base, double* acc_sum, int grid)
+void launch_update_t(su2g_lattice* h, int mu, int par, uint32_t sweep, const uint32_t* base, double* acc_sum, int grid,
+                     DD* plaq_part)
 {
     Field<R> U = make_field<R>(h->dirp, h->g.Vh);
     const R beta = (R)h->beta;
+    const int nt = update_block<KIND>();
+    cudaStream_t st = h->stream;
+    if (plaq_part) {   // parity-1 passes of MU >= 1 only
+        switch (mu) {
+            case 1: k_update<R, 1, KIND, true><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status, plaq_part); break;
+            case 2: k_update<R, 2, KIND, true><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status, plaq_part); break;
+            default: k_update<R, 3, KIND, true><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status, plaq_part); break;
+        }
+        return;
+    }
     switch (mu) {
-        case 0: k_update<R, 0, KIND><<<grid, update_block<KIND>(), 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
-        case 1: k_update<R, 1, KIND><<<grid, update_block<KIND>(), 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
-        case 2: k_update<R, 2, KIND><<<grid, update_block<KIND>(), 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
-        default: k_update<R, 3, KIND><<<grid, update_block<KIND>(), 0, h->stream>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        case 0: k_update<R, 0, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        case 1: k_update<R, 1, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        case 2: k_update<R, 2, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        default: k_update<R, 3, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
     }
 }
 
 }  // namespace
 
-int su2g::launch_update(su2g_lattice* h, int kind, int mu, int par, uint32_t sweep, double* acc_sum,
-                        const uint32_t* base)
+int su2g::update_grid(const su2g_lattice* h)
 {
+    return (int)((h->g.Vh + update_block<SU2G_HEATBATH>() - 1) / update_block<SU2G_HEATBATH>());
+}
+
+int su2g::update_plaq_parts(const su2g_lattice* h)
+{
+    return update_grid(h) * (update_block<SU2G_HEATBATH>() / 32);
+}
+
+int su2g::launch_update(su2g_lattice* h, int kind, int mu, int par, uint32_t sweep, double* acc_sum,
+                        const uint32_t* base, DD* plaq_part)
+{
+    static_assert(update_block<SU2G_HEATBATH>() == update_block<SU2G_OVERRELAX>(), "one grid for both kinds");
     const int cls = kind == SU2G_HEATBATH ? SU2G_K_HEATBATH : SU2G_K_OVERRELAX;
-    const int nt = kind == SU2G_HEATBATH ? update_block<SU2G_HEATBATH>() : update_block<SU2G_OVERRELAX>();
-    const int grid = (int)((h->g.Vh + nt - 1) / nt);
+    const int grid = update_grid(h);
+    if (plaq_part && (mu < 1 || par != 1))
+        return set_error(h, SU2G_EINVAL, "fused plaquette: only the parity-1 passes of mu >= 1 sum plaquettes");
     launch_begin(h, cls);
     if (h->prec == SU2G_FP32) {
-        if (kind == SU2G_HEATBATH) launch_update_t<float, SU2G_HEATBATH>(h, mu, par, sweep, base, acc_sum, grid);
-        else launch_update_t<float, SU2G_OVERRELAX>(h, mu, par, sweep, base, acc_sum, grid);
+        if (kind == SU2G_HEATBATH) launch_update_t<float, SU2G_HEATBATH>(h, mu, par, sweep, base, acc_sum, grid, plaq_part);
+        else launch_update_t<float, SU2G_OVERRELAX>(h, mu, par, sweep, base, acc_sum, grid, plaq_part);
     } else {
-        if (kind == SU2G_HEATBATH) launch_update_t<double, SU2G_HEATBATH>(h, mu, par, sweep, base, acc_sum, grid);
-        else launch_update_t<double, SU2G_OVERRELAX>(h, mu, par, sweep, base, acc_sum, grid);
+        if (kind == SU2G_HEATBATH) launch_update_t<double, SU2G_HEATBATH>(h, mu, par, sweep, base, acc_sum, grid, plaq_part);
+        else launch_update_t<double, SU2G_OVERRELAX>(h, mu, par, sweep, base, acc_sum, grid, plaq_part);
     }
     return launch_end(h, cls, kind == SU2G_HEATBATH ? "heatbath pass" : "overrelaxation pass");
 }
@@ -213,37 +264,72 @@ extern "C" int su2g_update_pass(su2g_lattice* h, int32_t kind, int32_t mu, int32
     return launch_update(h, kind, mu, parity, sweep, nullptr);
 }
 
-extern "C" int su2g_sweep(su2g_lattice* h, int32_t n_sweeps, int32_t n_hb, int32_t n_or, double* acc_out)
+int su2g::sweep_enqueue(su2g_lattice* h, int n_sweeps, int n_hb, int n_or, uint32_t sweep0, const uint32_t* base,
+                        double* acc_dev, int plaq_off)
 {
-    if (!h) return set_error(nullptr, SU2G_EINVAL, "su2g_sweep: null handle");
-    if (n_sweeps < 0 || n_hb < 0 || n_or < 0) return set_error(h, SU2G_EINVAL, "su2g_sweep: negative count");
+    const int parts = update_plaq_parts(h);   // per fused pass
+    const int subs = n_sweeps * (n_hb + n_or);
+    int rc = SU2G_OK;
+    if (plaq_off >= 0 && subs > 0 && (rc = ensure_partial_entries(h, 3 * (size_t)parts))) return rc;
+    int sub = 0;
+    for (int s = 0; s < n_sweeps; ++s)
+        for (int i = 0; i < n_hb + n_or; ++i) {
+            const bool hb = i < n_hb;
+            const bool last = ++sub == subs && plaq_off >= 0;
+            for (int mu = 0; mu < 4; ++mu)
+                for (int par = 0; par < 2; ++par) {
+                    DD* part = last && mu >= 1 && par == 1 ? h->partials + (size_t)(mu - 1) * parts : nullptr;
+                    rc = hb ? launch_update(h, SU2G_HEATBATH, mu, par, sweep0 + (uint32_t)(s * n_hb + i), acc_dev, base, part)
+                            : launch_update(h, SU2G_OVERRELAX, mu, par, 0u, nullptr, nullptr, part);
+                    if (rc) return rc;
+                }
+        }
+    if (plaq_off < 0) return SU2G_OK;
+    if (subs == 0) return plaquette_enqueue(h, plaq_off);
+    // the partials of the passes (1, 1), (2, 1), (3, 1): 6V plaquettes, (1/2) Re tr each
+    return finalize(h, 3 * parts, 1, 1.0 / (6.0 * (double)h->g.V), plaq_off);
+}
+
+namespace {
+
+int sweep_call(su2g_lattice* h, int32_t n_sweeps, int32_t n_hb, int32_t n_or, double* plaq_out, double* acc_out,
+               const char* who)
+{
+    if (!h) return set_error(nullptr, SU2G_EINVAL, "%s: null handle", who);
+    if (n_sweeps < 0 || n_hb < 0 || n_or < 0) return set_error(h, SU2G_EINVAL, "%s: negative count", who);
     cudaSetDevice(h->device);
     double* acc_dev = nullptr;
-    const int slot = 0;
+    const int slot_acc = 0, slot_plaq = 1;
     int rc = SU2G_OK;
     if (acc_out) {
-        acc_dev = h->d_out + slot;
+        acc_dev = h->d_out + slot_acc;
         if ((rc = check_cuda(h, cudaMemsetAsync(acc_dev, 0, sizeof(double), h->stream), "clearing acceptance")))
             return rc;
     }
-    for (int s = 0; s < n_sweeps; ++s) {
-        for (int i = 0; i < n_hb; ++i) {
-            for (int mu = 0; mu < 4; ++mu)
-                for (int par = 0; par < 2; ++par)
-                    if ((rc = launch_update(h, SU2G_HEATBATH, mu, par, h->hb_sweeps, acc_dev))) return rc;
-            h->hb_sweeps++;
-        }
-        for (int i = 0; i < n_or; ++i)
-            for (int mu = 0; mu < 4; ++mu)
-                for (int par = 0; par < 2; ++par)
-                    if ((rc = launch_update(h, SU2G_OVERRELAX, mu, par, 0u, nullptr))) return rc;
-    }
-    if (acc_out) {
-        if ((rc = fetch_results(h, slot, 1))) return rc;
+    rc = sweep_enqueue(h, n_sweeps, n_hb, n_or, h->hb_sweeps, nullptr, acc_dev, plaq_out ? slot_plaq : -1);
+    if (rc) return rc;
+    h->hb_sweeps += (uint32_t)(n_sweeps * n_hb);
+    if (acc_out || plaq_out) {
+        if ((rc = fetch_results(h, slot_acc, 2))) return rc;
         const double nupd = (double)n_sweeps * n_hb * 4.0 * (double)h->g.V;
-        *acc_out = nupd > 0 ? h->h_out[slot] / nupd : 0.0;
+        if (acc_out) *acc_out = nupd > 0 ? h->h_out[slot_acc] / nupd : 0.0;
+        if (plaq_out) *plaq_out = h->h_out[slot_plaq];
     }
     return SU2G_OK;
+}
+
+}  // namespace
+
+extern "C" int su2g_sweep(su2g_lattice* h, int32_t n_sweeps, int32_t n_hb, int32_t n_or, double* acc_out)
+{
+    return sweep_call(h, n_sweeps, n_hb, n_or, nullptr, acc_out, "su2g_sweep");
+}
+
+extern "C" int su2g_sweep_plaquette(su2g_lattice* h, int32_t n_sweeps, int32_t n_hb, int32_t n_or, double* plaq,
+                                    double* acc_out)
+{
+    if (h && !plaq) return set_error(h, SU2G_EINVAL, "su2g_sweep_plaquette: null plaquette output");
+    return sweep_call(h, n_sweeps, n_hb, n_or, plaq, acc_out, "su2g_sweep_plaquette");
 }
 
 extern "C" int su2g_gauge_update(su2g_lattice* h, int32_t nup, int32_t utype, int32_t stype, double eps, int32_t hits,

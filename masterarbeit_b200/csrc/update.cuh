@@ -65,9 +65,11 @@ __device__ __forceinline__ double kp_clamp(double d) { return d; }
 // All 18 links are loaded before the first product, so that a thread keeps every load of its
 // staple in flight at once (the pass is bound by memory latency x parallelism, not by ALU).  Each
 // term's last product accumulates into A inside its multiply-adds (24 fewer additions a link: the
-// FP64 heatbath pass 169 -> 155 us at 48^4 on B200).
-template <typename R, int MU, typename F = Field<R>>
-__device__ __forceinline__ Q<R> staple_update(const F& U, const Geom& g, const Site& s, int par)
+// FP64 heatbath pass 169 -> 155 us at 48^4 on B200).  With NLOW > 0, *low receives the partial sum
+// of the first NLOW terms (nu = 0 .. NLOW-1 for NLOW <= MU), taken from the same accumulation, so A
+// is the same either way.
+template <typename R, int MU, int NLOW = 0, typename F = Field<R>>
+__device__ __forceinline__ Q<R> staple_update(const F& U, const Geom& g, const Site& s, int par, Q<R>* low = nullptr)
 {
     const int q = par ^ 1;
     const int dmu = up_off<MU>(g, s);
@@ -90,6 +92,7 @@ __device__ __forceinline__ Q<R> staple_update(const F& U, const Geom& g, const S
     for (int k = 0; k < 3; ++k) {
         A = q_mul_nd_add(A, q_mul_nd(a[k], b[k]), c[k]);
         A = q_mul_dn_add(A, q_mul(e[k], d[k]), f[k]);
+        if (k + 1 == NLOW) *low = A;
     }
     return A;
 }

@@ -84,6 +84,7 @@ _SIGS = {
     "su2g_upload_aos_f64": (ctypes.c_int, [_P, _DP]),
     "su2g_download_aos_f64": (ctypes.c_int, [_P, _DP]),
     "su2g_sweep": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP]),
+    "su2g_sweep_plaquette": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]),
     "su2g_update_pass": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]),
     "su2g_graph_run": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]),
     "su2g_graph_release": (ctypes.c_int, [_P]),
@@ -265,6 +266,14 @@ class Lattice:
             return v.value
         self._check(self.lib.su2g_sweep(self.h, n_sweeps, n_hb, n_or, None))
         return None
+
+    def sweep_plaquette(self, n_sweeps=1, n_hb=1, n_or=0, acc=False):
+        """sweep() and the plaquette of the resulting field, summed inside the last sweep's update
+        passes; returns the plaquette, or (plaquette, acceptance) with acc=True."""
+        p, a = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.su2g_sweep_plaquette(self.h, n_sweeps, n_hb, n_or, ctypes.byref(p),
+                                                  ctypes.byref(a) if acc else None))
+        return (p.value, a.value) if acc else p.value
 
     def gauge_update(self, nup=1, utype=1, stype=0, eps=0.15, hits=1):
         """gaugefieldUpdate(iup, nup, utype, stype): utype 1 heatbath / 0 Metropolis (step eps,

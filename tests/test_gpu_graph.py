@@ -1,7 +1,7 @@
 """su2g_graph_run (the qcd.c:55-60 update/measure loop as one replayed CUDA graph) against the same
-su2g_sweep / su2g_plaquette sequence issued call by call: identical fields and plaquette traces,
-the Philox sweep counter carried across calls, and a new capture whenever the field's buffers
-(APE ping-pong), beta or the block shape change."""
+su2g_sweep_plaquette sequence issued call by call: identical fields and plaquette traces (and the
+plaquette kernel's value to rounding), the Philox sweep counter carried across calls, and a new
+capture whenever the field's buffers (APE ping-pong), beta or the block shape change."""
 import numpy as np
 import pytest
 
@@ -13,8 +13,11 @@ pytestmark = pytest.mark.gpu
 def _plain(L, n_blocks, every, n_hb, n_or):
     plaq, acc = [], []
     for _ in range(n_blocks):
-        acc.append(L.sweep(every, n_hb, n_or, acc=True))
-        plaq.append(L.plaquette())
+        p, a = L.sweep_plaquette(every, n_hb, n_or, acc=True)
+        # the sum inside the update passes against the plaquette kernel on the same field
+        assert abs(p - L.plaquette()) <= (1e-14 if L.precision == "fp64" else 5e-7) * abs(p)
+        plaq.append(p)
+        acc.append(a)
     return np.array(plaq), np.array(acc)
 
 

@@ -45,6 +45,7 @@ def test_null_handle_is_an_error_not_a_crash():
     v = ctypes.c_double()
     assert lib.su2g_plaquette(None, ctypes.byref(v)) == -1
     assert lib.su2g_sweep(None, 1, 1, 0, None) == -1
+    assert lib.su2g_sweep_plaquette(None, 1, 1, 0, ctypes.byref(v), None) == -1
 
 
 @pytest.mark.parametrize("name", ["cfg_4x4x4x4_base.cfg", "cfg_6x4x4x8_base.cfg", "cfg_8x8x8x8_base.cfg"])

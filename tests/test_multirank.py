@@ -76,7 +76,7 @@ class FakeLattice:
     profiled pass reports one event-timed launch per call and kernel class."""
 
     def __init__(self, dims, **kw):
-        self.calls = {"heatbath": 0, "plaquette": 0}
+        self.calls = {"heatbath": 0, "plaquette": 0, "reduce": 0}
         self.profiling = False
 
     def sweep(self, n_sweeps=1, n_hb=1, n_or=0, acc=False):
@@ -85,6 +85,11 @@ class FakeLattice:
     def plaquette(self):
         self.calls["plaquette"] += 1
         return 0.5
+
+    def sweep_plaquette(self, n_sweeps=1, n_hb=1, n_or=0, acc=False):
+        self.sweep(n_sweeps, n_hb, n_or)
+        self.calls["reduce"] += 1
+        return (0.5, 0.98) if acc else 0.5
 
     def synchronize(self):
         pass
