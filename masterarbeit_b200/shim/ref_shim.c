@@ -47,6 +47,8 @@ static int g_state = HOST_NEWER;
 static int g_prec = SU2G_FP64;
 static int g_nor = 0;
 static int g_io = 0;                 /* > 0 inside a wrapped readConfig / writeConfig */
+static double g_plaq = 0.0;          /* plaquette of the device field summed by the last sweep */
+static int g_plaq_ok = 0;            /* g_plaq is the current field's (no change since that sweep) */
 
 static void check(int rc, su2g_lattice *h, const char *where)
 {
@@ -105,6 +107,7 @@ static void to_device(void)
     if (g_state == HOST_NEWER) {
         check(su2g_upload_aos_f64(g_h, (const double *)pu[0][0]), g_h, "su2g_upload_aos_f64 [ref_shim.c]");
         g_state = IN_SYNC;
+        g_plaq_ok = 0;
     }
 }
 
@@ -119,7 +122,9 @@ static void to_host(void)
 /* gaugefieldUpdate, modules/update/update.c:102-175: nup sweeps of the heatbath (utype 1) or of
  * Metropolis with step runParams.eps (utype 0), every link once (stype 0) or random site
  * selection (stype 1); heatbath sequential sweeps are followed by SU2G_OR overrelaxation sweeps
- * each.  Reprojection on every store, the same log lines. */
+ * each.  Reprojection on every store, the same log lines.  Heatbath sequential sweeps run as
+ * su2g_sweep_plaquette, which also sums the plaquette of the new field inside its update passes:
+ * the plaquette() that main/qcd.c calls next (qcd.c:55-60) returns it without another kernel. */
 void gaugefieldUpdate(int iup, int nup, int utype, int stype)
 {
     double acc = 0.0, t1, t2;
@@ -132,11 +137,14 @@ void gaugefieldUpdate(int iup, int nup, int utype, int stype)
     to_device();
     check(su2g_set_beta(g_h, runParams.beta), g_h, "su2g_set_beta [ref_shim.c]");
     t1 = getTime();
-    if (utype == 1 && stype == 0)
-        check(su2g_sweep(g_h, nup, 1, g_nor, &acc), g_h, "su2g_sweep [ref_shim.c]");
-    else
+    g_plaq_ok = 0;
+    if (utype == 1 && stype == 0) {
+        check(su2g_sweep_plaquette(g_h, nup, 1, g_nor, &g_plaq, &acc), g_h, "su2g_sweep_plaquette [ref_shim.c]");
+        g_plaq_ok = 1;
+    } else {
         check(su2g_gauge_update(g_h, nup, utype, stype, runParams.eps, 1, &acc), g_h,
               "su2g_gauge_update [ref_shim.c]");
+    }
     t2 = getTime();
     g_state = DEVICE_NEWER;
 
@@ -161,6 +169,7 @@ double plaquette(void)
         check(su2g_plaquette(g_chk, &p), g_chk, "su2g_plaquette [ref_shim.c]");
         return p;
     }
+    if (g_plaq_ok && g_h && g_state == DEVICE_NEWER) return g_plaq;
     to_device();
     check(su2g_plaquette(g_h, &p), g_h, "su2g_plaquette [ref_shim.c]");
     return p;
@@ -178,6 +187,7 @@ static void smear(int ns, double sp, sun_mat *u[VOL][DIM], int mode)
     to_device();
     check(su2g_ape(g_h, ns, sp, mode), g_h, "su2g_ape [ref_shim.c]");
     g_state = DEVICE_NEWER;
+    g_plaq_ok = 0;
 }
 
 /* smearing_APE_all / _spatial / _temporal, modules/obs/smearing.c:74-168 */
@@ -221,6 +231,7 @@ double topologicalCharge(void)
 void readConfig(char *infile)
 {
     g_state = HOST_NEWER;
+    g_plaq_ok = 0;
     g_io++;
     ref_readConfig(infile);   /* its plaquette check uploads the new field in FP64 mode */
     g_io--;
@@ -230,6 +241,7 @@ void readConfig(char *infile)
 void readConfigForThermalisation(char *infile)
 {
     g_state = HOST_NEWER;
+    g_plaq_ok = 0;
     g_io++;
     ref_readConfigForThermalisation(infile);
     g_io--;

@@ -34,7 +34,7 @@ def test_dropin_links_the_shim():
     syms = subprocess.run(["nm", os.path.join(DROPIN, "qcd")], capture_output=True, text=True).stdout
     assert re.search(r" T gaugefieldUpdate$", syms, re.M)
     assert re.search(r" T plaquette$", syms, re.M)
-    assert re.search(r" U su2g_sweep$", syms, re.M)
+    assert re.search(r" U su2g_sweep_plaquette$", syms, re.M)
     assert not re.search(r" T localHeatbathUpdate$", syms, re.M)
     assert re.search(r" T ref_readConfig$", syms, re.M)
     dyn = subprocess.run(["ldd", os.path.join(DROPIN, "qcd")], capture_output=True, text=True).stdout
