@@ -222,15 +222,36 @@ __device__ __forceinline__ size_t wilson_slot(int r, int ti, int nT, int warp)
                                     : ((size_t)r * nT + ti) * (blockDim.x >> 5) + warp;
 }
 
-template <typename R>
-__device__ __forceinline__ void wilson_acc(double* __restrict__ wacc, R w, size_t slot, int lane)
+// The RC terms w[r] of one T into their slots.  FP64: each thread into its own slots.  FP32: the
+// warp sums of all RC terms by one transposing reduction (RC a power of two <= 32): at each of the
+// first log2(RC) shuffle levels a lane keeps one half of its values and sends the other half to its
+// partner, which keeps the opposite half, so the value count halves with the distance; a plain
+// butterfly over the remaining lane bits follows.  Lane r * (32 / RC) then holds the warp sum of
+// term r, after RC - 1 + 5 - log2(RC) shuffles and adds (6 for RC = 4; one butterfly per term took
+// 5 RC = 20).
+template <typename R, int RC>
+__device__ __forceinline__ void wilson_acc(double* __restrict__ wacc, R (&w)[RC], int ti, int nT, int warp, int lane)
 {
     if (wilson_thread_slots<R>()) {
-        wacc[slot] += (double)w;
-    } else {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-        if (lane == 0) wacc[slot] += (double)w;
+        for (int r = 0; r < RC; ++r) wacc[wilson_slot<R>(r, ti, nT, warp)] += (double)w[r];
+    } else {
+        static_assert(RC >= 1 && RC <= 32 && (RC & (RC - 1)) == 0, "RC must be a power of two <= 32");
+#pragma unroll
+        for (int n = RC, width = 16; n > 1; n >>= 1, width >>= 1) {
+            const bool upper = (lane & width) != 0;
+#pragma unroll
+            for (int i = 0; i < n / 2; ++i) {
+                const R keep = upper ? w[i + n / 2] : w[i];
+                const R send = upper ? w[i] : w[i + n / 2];
+                w[i] = keep + __shfl_xor_sync(0xffffffffu, send, width);
+            }
+        }
+        R x = w[0];
+#pragma unroll
+        for (int width = 16 / RC; width > 0; width >>= 1) x += __shfl_xor_sync(0xffffffffu, x, width);
+        constexpr int group = 32 / RC;
+        if ((lane & (group - 1)) == 0) wacc[wilson_slot<R>(lane / group, ti, nT, warp)] += (double)x;
     }
 }
 
@@ -274,11 +295,10 @@ __device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g,
 #pragma unroll
         for (int r = 0; r < RC; ++r) Y[r] = q_mul_nd(q_mul(UT, buf[(size_t)r * nt + up]), UR[r]);
         if (T < tlo) continue;
+        R w[RC];
 #pragma unroll
-        for (int r = 0; r < RC; ++r) {
-            const R w = valid ? q_dot(Y[r], SX[r]) : R(0);
-            wilson_acc<R>(wacc, w, wilson_slot<R>(r, T - tlo, nT, warp), lane);
-        }
+        for (int r = 0; r < RC; ++r) w[r] = valid ? q_dot(Y[r], SX[r]) : R(0);
+        wilson_acc<R, RC>(wacc, w, T - tlo, nT, warp, lane);
     }
     __syncthreads();   // the buffers are written again by the next direction
 }
