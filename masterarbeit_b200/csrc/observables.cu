@@ -390,9 +390,13 @@ __global__ void __launch_bounds__(kBlock) k_lines(Field<R> U, Field<R> L2, Field
 // Offset of the lexicographic index for k steps (|k| <= 3) along direction d from coordinate c.
 __device__ __forceinline__ int shift_by(const Geom& g, int d, int c, int k)
 {
+    const int L = g.L[d];
     int cc = c + k;
-    while (cc < 0) cc += g.L[d];
-    while (cc >= g.L[d]) cc -= g.L[d];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {   // |k| <= 3 <= 2 L - 1 for L >= 2: two wraps at most
+        cc += cc < 0 ? L : 0;
+        cc -= cc >= L ? L : 0;
+    }
     return (cc - c) * g.S[d];
 }
 

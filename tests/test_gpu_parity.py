@@ -86,12 +86,13 @@ def test_qtop_after_ape(golden, lat):
                 assert abs(q - qref) <= tol * sabs, (prec, N, q, qref, sabs)
 
 
-@pytest.mark.parametrize("dims", [(4, 4, 6, 6), (6, 6, 4, 10), (4, 6, 8, 10)])
+@pytest.mark.parametrize("dims", [(4, 4, 6, 6), (6, 6, 4, 10), (4, 6, 8, 10), (2, 4, 6, 4)])
 def test_ape_and_qtop_on_ragged_geometries(dims):
     """Half volumes that are not whole multiples of a CTA's run of sites (288 and 720 against the
     64 sites of a 128-thread CTA whose warps alternate parity; 960 against the 128 sites of the
     FP64 CTAs), so the last CTA of the APE and charge kernels is partly empty: APE in every mode,
-    then Q, against the oracle on the same uploaded Haar field, in FP64 and FP32."""
+    then Q, against the oracle on the same uploaded Haar field, in FP64 and FP32.  An extent of 2
+    makes the charge's 3-link offsets wrap twice."""
     U = O.start(dims, "haar", 17)
     for mode in ("all", "spatial", "temporal"):
         ref = O.ape(dims, U, 3, 0.4, mode)
