@@ -101,14 +101,16 @@ template <int K>
 __device__ __forceinline__ int shift_k(const Geom& g, int ck, int j)
 {
     int c = ck + j;
-    while (c >= g.L[K]) c -= g.L[K];
+    c -= c >= g.L[K] ? g.L[K] : 0;
+    if (c >= g.L[K]) c %= g.L[K];   // j >= L_K: a loop longer than the lattice
     return (c - ck) * g.S[K];
 }
 
 __device__ __forceinline__ int shift_t(const Geom& g, int ct, int T)
 {
     int c = ct + T;
-    while (c >= g.L[0]) c -= g.L[0];
+    c -= c >= g.L[0] ? g.L[0] : 0;
+    if (c >= g.L[0]) c %= g.L[0];   // T >= L_t does not occur (T <= L_t - 1 is checked)
     return (c - ct) * g.S[0];
 }
 
