@@ -41,8 +41,10 @@ __device__ __forceinline__ float kp_sqrt(float x)
     return r;
 }
 __device__ __forceinline__ double kp_sqrt(double x) { return sqrt(x); }
-// 1/|A| and 1/(beta |A|) from |A|^2: FP32 from one hardware reciprocal square root.  |A| = 0 gives
-// k = NaN (0 * inf), which fails the k > eps test like k = 0 does.
+// 1/|A| and 1/(beta |A|) from |A|^2, from one reciprocal square root (FP32: the hardware
+// approximation; FP64: rsqrt, within an ulp, in place of a square root and two divisions: the FP64
+// heatbath pass 152.9 -> 152.1 us at 48^4).  |A| = 0 gives k = NaN (0 * inf), which fails the
+// k > eps test like k = 0 does.
 __device__ __forceinline__ void kp_norms(float n2, float beta, float& k, float& ik, float& ia)
 {
     ik = rsqrtf(n2);
@@ -51,9 +53,9 @@ __device__ __forceinline__ void kp_norms(float n2, float beta, float& k, float& 
 }
 __device__ __forceinline__ void kp_norms(double n2, double beta, double& k, double& ik, double& ia)
 {
-    k = sqrt(n2);
-    ik = 1.0 / k;
-    ia = 1.0 / (k * beta);
+    ik = rsqrt(n2);
+    k = n2 * ik;
+    ia = ik / beta;
 }
 // The FP32 logs of uniforms just below 1 may come out positive by their absolute error (~2^-21);
 // delta is clamped at 0 so that sqrt(delta (2 - delta)) stays real.  FP64 logs are exact in sign.
