@@ -39,6 +39,42 @@ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1)
     return c;
 }
 
+// The ten round keys of a seed, computed once on the host: a kernel that takes them as a parameter
+// reads them from the constant bank inside each round instead of adding the Weyl increments per
+// block (the same words, so the same draws).
+struct PhiloxKeys {
+    uint32_t k0[10], k1[10];
+};
+
+inline PhiloxKeys philox_keys(uint64_t seed)
+{
+    PhiloxKeys K;
+    uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    for (int r = 0; r < 10; ++r) {
+        K.k0[r] = k0;
+        K.k1[r] = k1;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return K;
+}
+
+__device__ __forceinline__ U4 philox4x32_10(U4 c, const PhiloxKeys& K)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        U4 n;
+        n.x = hi1 ^ c.y ^ K.k0[r];
+        n.y = lo1;
+        n.z = hi0 ^ c.w ^ K.k1[r];
+        n.w = lo0;
+        c = n;
+    }
+    return c;
+}
+
 // Stream kinds: heatbath/fallback draws, starts, Metropolis hits, random-order visit counts.
 enum : uint32_t { kStreamUpdate = 0u, kStreamStart = 1u, kStreamMetro = 2u, kStreamVisit = 3u };
 
@@ -51,6 +87,17 @@ __device__ __forceinline__ U4 link_random(uint64_t seed, uint32_t site, uint32_t
     c.z = (draw << 3) | (dir << 1) | tag;
     c.w = (kind << 24) | replica;
     return philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+__device__ __forceinline__ U4 link_random(const PhiloxKeys& K, uint32_t site, uint32_t sweep, uint32_t dir,
+                                          uint32_t draw, uint32_t tag, uint32_t kind, uint32_t replica)
+{
+    U4 c;
+    c.x = site;
+    c.y = sweep;
+    c.z = (draw << 3) | (dir << 1) | tag;
+    c.w = (kind << 24) | replica;
+    return philox4x32_10(c, K);
 }
 
 // Uniforms in the open interval (0,1).  FP64 keeps all 32 bits; FP32 keeps the top 23 bits, so the

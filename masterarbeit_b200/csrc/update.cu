@@ -40,7 +40,7 @@ constexpr int update_block() { return 128; }
 // staple_update (U A = the sum of the plaquettes through U); the separate plaquette kernel
 // (plaquette.c:67-100) then need not run.
 template <typename R, int MU, int KIND, bool PLQ = false>
-__global__ void __launch_bounds__(update_block<KIND>(), 1024 / update_block<KIND>()) k_update(Field<R> U, Geom g, int par, R beta, uint64_t seed, uint32_t sweep,
+__global__ void __launch_bounds__(update_block<KIND>(), 1024 / update_block<KIND>()) k_update(Field<R> U, Geom g, int par, R beta, PhiloxKeys seed, uint32_t sweep,
                                                    const uint32_t* __restrict__ sweep_base, uint32_t replica,
                                                    double* __restrict__ acc_sum, unsigned* __restrict__ status,
                                                    DD* __restrict__ plaq_part = nullptr)
@@ -174,19 +174,20 @@ void launch_update_t(su2g_lattice* h, int mu, int par, uint32_t sweep, const uin
     const R beta = (R)h->beta;
     const int nt = update_block<KIND>();
     cudaStream_t st = h->stream;
+    const PhiloxKeys keys = philox_keys(h->seed);
     if (plaq_part) {   // parity-1 passes of MU >= 1 only
         switch (mu) {
-            case 1: k_update<R, 1, KIND, true><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status, plaq_part); break;
-            case 2: k_update<R, 2, KIND, true><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status, plaq_part); break;
-            default: k_update<R, 3, KIND, true><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status, plaq_part); break;
+            case 1: k_update<R, 1, KIND, true><<<grid, nt, 0, st>>>(U, h->g, par, beta, keys, sweep, base, h->replica, acc_sum, h->d_status, plaq_part); break;
+            case 2: k_update<R, 2, KIND, true><<<grid, nt, 0, st>>>(U, h->g, par, beta, keys, sweep, base, h->replica, acc_sum, h->d_status, plaq_part); break;
+            default: k_update<R, 3, KIND, true><<<grid, nt, 0, st>>>(U, h->g, par, beta, keys, sweep, base, h->replica, acc_sum, h->d_status, plaq_part); break;
         }
         return;
     }
     switch (mu) {
-        case 0: k_update<R, 0, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
-        case 1: k_update<R, 1, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
-        case 2: k_update<R, 2, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
-        default: k_update<R, 3, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, h->seed, sweep, base, h->replica, acc_sum, h->d_status); break;
+        case 0: k_update<R, 0, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, keys, sweep, base, h->replica, acc_sum, h->d_status); break;
+        case 1: k_update<R, 1, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, keys, sweep, base, h->replica, acc_sum, h->d_status); break;
+        case 2: k_update<R, 2, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, keys, sweep, base, h->replica, acc_sum, h->d_status); break;
+        default: k_update<R, 3, KIND><<<grid, nt, 0, st>>>(U, h->g, par, beta, keys, sweep, base, h->replica, acc_sum, h->d_status); break;
     }
 }
 

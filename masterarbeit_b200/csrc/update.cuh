@@ -125,8 +125,9 @@ __device__ __forceinline__ Q<R> fallback_link(R r0, R r1, R r2)
 // `draw_base` (visit << kVisitShift) separates the draws of repeated visits in a random-order sweep.
 constexpr int kVisitShift = 21;   // above every trial index (kMaxTrials = 2^20)
 
-template <typename R>
-__device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, uint64_t seed, uint32_t site, uint32_t sweep,
+// `seed` is the 64-bit seed or its precomputed round keys (PhiloxKeys): the same draws either way.
+template <typename R, typename Seed>
+__device__ __forceinline__ bool heatbath_link(const Q<R>& A, R beta, const Seed& seed, uint32_t site, uint32_t sweep,
                                               uint32_t mu, uint32_t replica, uint32_t& trials, Q<R>& out,
                                               unsigned* status, uint32_t draw_base = 0u)
 {
