@@ -102,7 +102,8 @@ __device__ __forceinline__ U4 link_random(const PhiloxKeys& K, uint32_t site, ui
 
 // Uniforms in the open interval (0,1).  FP64 keeps all 32 bits; FP32 keeps the top 23 bits, so the
 // FP32 and FP64 chains consume identical Philox words and differ only by the conversion.
-__device__ __forceinline__ double u01(uint32_t w, double) { return ((double)w + 0.5) * (1.0 / 4294967296.0); }
+// FP64: (w + 1/2) / 2^32 as one multiply-add; w 2^-32 and the sum are exact, so the value is the same
+__device__ __forceinline__ double u01(uint32_t w, double) { return fma((double)w, 1.0 / 4294967296.0, 0.5 / 4294967296.0); }
 __device__ __forceinline__ float u01(uint32_t w, float)
 {
     // ((w >> 9) + 1/2) / 2^23 as one multiply-add: both forms are exact, so the value is the same
