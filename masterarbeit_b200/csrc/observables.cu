@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kBlock) k_wilson(Field<R> U, Geom g, int r0, i
 // line at x + T t that the loop needs for every T is the one the thread of slice t + T stored:
 // it is read, not rebuilt, which removes the longest product chain of the per-site form.
 constexpr int kWilsonColMaxThreads = 512;
-constexpr int kWilsonRc8MaxThreads = 192;   // the FP32 column kernel with eight loops a thread
+constexpr int kWilsonRc8MaxThreads = 192;   // the column kernel with eight (FP32) / four (FP64) loops
 
 // Accumulation of the column kernel's loop terms in shared memory.  FP32: the 32 lanes' terms are
 // summed in the link precision (one shuffle per step; its rounding, ~1e-7 of a warp sum, is far
@@ -306,11 +306,12 @@ __device__ __forceinline__ void wilson_col_dir(const Field<R>& U, const Geom& g,
     __syncthreads();   // the buffers are written again by the next direction
 }
 
-// FP32 with eight loops a thread (167 registers) is capped at kWilsonRc8MaxThreads threads (96-thread
-// CTAs at 48^4) so that it need not spill: the R <= 9 set in two launches took 3.95 ms against
-// 4.25 ms in three of four loops.  Eight loops are chosen only where a column fits the cap.
+// FP32 with eight loops a thread (167 registers) and FP64 with four (162) are capped at
+// kWilsonRc8MaxThreads threads (96-thread CTAs at 48^4) so that they need not spill: the R <= 9 set
+// took 3.95 ms against 4.25 ms with four loops (FP32) and 9.87 against 10.10 ms with two loops in
+// 288-thread CTAs (FP64).  These widths are chosen only where a column fits the cap.
 template <typename R, int RC>
-__global__ void __launch_bounds__(sizeof(R) == 4 && RC >= 8 ? kWilsonRc8MaxThreads : kWilsonColMaxThreads, 1) k_wilson_col(Field<R> U, Geom g, int sw, int r0, int tlo,
+__global__ void __launch_bounds__((sizeof(R) == 4 && RC >= 8) || (sizeof(R) == 8 && RC >= 4) ? kWilsonRc8MaxThreads : kWilsonColMaxThreads, 1) k_wilson_col(Field<R> U, Geom g, int sw, int r0, int tlo,
                                                                         int thi, DD* __restrict__ partials)
 {
     extern __shared__ __align__(16) unsigned char wsm[];
@@ -515,7 +516,7 @@ template <typename R, int RC>
 int launch_wilson_t(su2g_lattice* h, void* const dirs[4], int r0, int tlo, int thi)
 {
     const Field<R> U = make_field<R>(dirs, h->g.Vh);
-    const int sw = wilson_col_width(h->g, sizeof(R) == 4 && RC >= 4 ? 64 : 256);
+    const int sw = wilson_col_width(h->g, (sizeof(R) == 4 && RC >= 4) || (sizeof(R) == 8 && RC >= 4) ? 64 : 256);
     if (sw > 0) {
         const int threads = sw * h->g.L[0];
         const size_t smem = wilson_col_smem<R, RC>(threads, thi - tlo + 1);
@@ -714,7 +715,7 @@ int su2g::wilson_enqueue(su2g_lattice* h, void* const dirs[4], const int32_t* R,
     // 22.5 ms against 11.2 ms for W(R, T <= 9) at 48^4); the per-site kernel prefers 8
     const int sw8 = wilson_col_width(h->g, 64);
     const bool rc8 = sw8 > 0 && sw8 * h->g.L[0] <= kWilsonRc8MaxThreads;
-    const int rc_max = wilson_col_width(h->g) > 0 ? (h->prec == SU2G_FP32 ? (rc8 ? 8 : 4) : 2) : 8;
+    const int rc_max = wilson_col_width(h->g) > 0 ? (h->prec == SU2G_FP32 ? (rc8 ? 8 : 4) : (rc8 ? 4 : 2)) : 8;
     for (int r0 = 1; r0 <= rmax;) {
         const int left = rmax - r0 + 1;
         const int rc_n = left >= 8 && rc_max >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
