@@ -59,16 +59,17 @@ __global__ void __launch_bounds__(128, 8) k_plaquette(Field<R> U, Geom g, DD* __
 
 // One Jacobi step U'_mu(x) = Proj(U_mu(x) + alpha S_mu(x)) (smearing.c:74-168) with the staple
 // sums of ape_staples (ape.cuh).  Reads `in`, writes only the updated directions of `out`.
-// 128-thread CTAs; resident CTAs per SM, measured at 48^4 on B200: FP32 APE_all five (at most 102
-// registers; 239 us against 254 us with two 256-thread CTAs, 243 us with six); FP32 spatial and
-// temporal eight (131.4 us spatial against 132.6 us with four of 256 and 164 us with two). FP64
+// 128-thread CTAs; resident CTAs per SM, measured at 48^4 on B200: FP32 APE_all four (at most 128
+// registers; 235.5 us against 238.8 us with five, 243 us with six, 254 us with two 256-thread
+// CTAs); FP32 spatial and temporal eight (131.4 us spatial against 132.6 us with four of 256, 136 us
+// with six, 164 us with two). FP64
 // APE_all three (619 us against 626 us with four, 655 us with two of 256), spatial four (337 us
 // against 359 us with three, 357 us with two of 256), temporal eight (212 against 216 us with four
 // of 256).
 template <typename R, int MODE>
 constexpr int ape_min_blocks()
 {
-    return MODE == SU2G_APE_ALL ? (sizeof(R) == 4 ? 5 : 3) : (sizeof(R) == 4 || MODE == SU2G_APE_TEMPORAL ? 8 : 4);
+    return MODE == SU2G_APE_ALL ? (sizeof(R) == 4 ? 4 : 3) : (sizeof(R) == 4 || MODE == SU2G_APE_TEMPORAL ? 8 : 4);
 }
 template <typename R, int MODE>
 constexpr int ape_block()
